@@ -1,0 +1,1211 @@
+/*
+ * api.cu — host side of the C ABI (include/adds.h).
+ *
+ * Replaces the reference host driver gg_main (ads_int/kernel.cu:185-288) and
+ * the host half of the worklist (wl.h:203-460): sizing and allocation of the
+ * bucket pool, per-solve reset, the delta choice (profiler_kernel + set_param,
+ * kernel.cu:153-183 / wl.h:395-449), the launch, timing, and the work count.
+ * Differences by design: errors are return codes (no exit/assert), the pool
+ * regrows and the solve reruns when the device reports overflow, and the
+ * launch is one cooperative persistent kernel instead of CDP children.
+ */
+#include <cuda_runtime.h>
+#include <errno.h>
+#include <fcntl.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/adds.h"
+#include "adds_internal.h"
+
+/* engine.cu */
+cudaError_t adds_engine_prepare(bool flt, int *max_blocks_per_sm, int *block);
+cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStream_t st);
+cudaError_t adds_engine_launch_solve(const EngParams &P, cudaStream_t st);
+cudaError_t adds_engine_launch_reached(const unsigned *row, const unsigned *dist, unsigned n,
+                                       unsigned inf, unsigned long long *out, cudaStream_t st);
+cudaError_t adds_engine_launch_reset(unsigned long long *fq, unsigned fq_cells,
+                                     unsigned pool_pages, unsigned *hub_seq, unsigned hub_cells,
+                                     cudaStream_t st);
+/* gen.cu */
+int adds_gen_build(const adds_gen_spec *sp, unsigned **row_out, uint2 **edges_out,
+                   uint32_t *n_out, uint64_t *m_out, cudaStream_t st);
+/* adjoint.cu */
+int adds_adjoint_run(struct AdjointJob *job);
+
+/* ------------------------------------------------------------------------ */
+static thread_local char g_last_err[256] = "";
+
+static int cuda_fail(cudaError_t e, const char *what) {
+  snprintf(g_last_err, sizeof g_last_err, "%s: %s", what, cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return ADDS_ERR_OOM;
+  }
+  cudaGetLastError();
+  return ADDS_ERR_CUDA;
+}
+#define CK(x)                                      \
+  do {                                             \
+    cudaError_t _e = (x);                          \
+    if (_e != cudaSuccess) return cuda_fail(_e, #x); \
+  } while (0)
+
+extern "C" int adds_abi_version(void) { return ADDS_ABI_VERSION; }
+extern "C" const char *adds_last_cuda_error(void) { return g_last_err; }
+
+extern "C" const char *adds_strerror(int code) {
+  switch (code) {
+    case ADDS_OK: return "ok";
+    case ADDS_ERR_INVALID: return "invalid argument";
+    case ADDS_ERR_IO: return "i/o error";
+    case ADDS_ERR_FORMAT: return "malformed graph file";
+    case ADDS_ERR_OOM: return "out of memory";
+    case ADDS_ERR_CUDA: return "CUDA runtime error";
+    case ADDS_ERR_DEVICE_TIMEOUT: return "bounded device wait timed out";
+    case ADDS_ERR_WL_OVERFLOW: return "worklist pool exhausted";
+    case ADDS_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case ADDS_ERR_UNSUPPORTED: return "unsupported request";
+    default: return "unknown error";
+  }
+}
+
+extern "C" void adds_opts_init(adds_opts *o) {
+  if (!o) return;
+  memset(o, 0, sizeof *o);
+  o->delta_shift = -1;
+  o->delta_scale = 0.f;
+  o->adapt = -1;
+  o->strict_order = -1;
+}
+
+static unsigned next_pow2(unsigned long long x) {
+  unsigned l = 0;
+  while ((1ull << l) < x) ++l;
+  return l;
+}
+
+/* ------------------------------------------------------------------------ */
+/* engine: the bucket pool and per-query queue state                         */
+struct EngQuery {
+  const unsigned *row;
+  const uint2 *edges;
+  unsigned *dist;
+  unsigned n;
+  unsigned long long m;
+  unsigned src;
+  float scale;
+  unsigned shift;
+  unsigned graph_id;
+};
+
+struct Engine {
+  int device = -1;
+  bool flt = false;
+  unsigned nq = 0;
+  unsigned pool_pages = 0, fq_cells = 0, max_n = 0;
+  unsigned long long *pool = nullptr;
+  unsigned *pgen = nullptr, *pcons = nullptr;
+  unsigned long long *fq = nullptr;
+  HubChunk *hub = nullptr;
+  unsigned *hub_seq = nullptr;
+  GlobalCtl *g = nullptr;
+  QueryDesc *qs = nullptr;
+  QueryCtl *ctl = nullptr;
+  SlotCtr *slots = nullptr;
+  unsigned long long *pt = nullptr;
+  unsigned long long *reach = nullptr;
+  GlobalCtl *g_host = nullptr; /* pinned */
+  std::vector<QueryDesc> qs_host;
+  size_t bytes = 0;
+  int block = 0, max_bps = 0, num_sms = 0;
+};
+
+static void engine_free(Engine &E) {
+  void *ptrs[] = {E.pool, E.pgen, E.pcons, E.fq, E.hub, E.hub_seq, E.g, E.qs, E.ctl, E.slots, E.pt, E.reach};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (E.g_host) cudaFreeHost(E.g_host);
+  E = Engine();
+}
+
+static int engine_full_reset(Engine &E, cudaStream_t st) {
+  const unsigned hub_cells = 1u << ADDS_HUB_RING_LOG2;
+  CK(cudaMemsetAsync(E.pool, 0, (size_t)E.pool_pages * ADDS_PAGE * 8, st));
+  CK(cudaMemsetAsync(E.pgen, 0, (size_t)E.pool_pages * 4, st));
+  CK(cudaMemsetAsync(E.pcons, 0, (size_t)E.pool_pages * 4, st));
+  CK(cudaMemsetAsync(E.g, 0, sizeof(GlobalCtl), st));
+  CK(cudaMemsetAsync(E.slots, 0, (size_t)E.nq * ADDS_NB * sizeof(SlotCtr), st));
+  CK(cudaMemsetAsync(E.ctl, 0, (size_t)E.nq * sizeof(QueryCtl), st));
+  size_t pt_words = 0;
+  for (auto &q : E.qs_host) pt_words += (size_t)ADDS_NB << q.ptn_log2;
+  CK(cudaMemsetAsync(E.pt, 0xFF, pt_words * 8, st));
+  const unsigned long long tail = E.pool_pages;
+  CK(cudaMemcpyAsync(&E.g->fq_tail, &tail, 8, cudaMemcpyHostToDevice, st));
+  CK(adds_engine_launch_reset(E.fq, E.fq_cells, E.pool_pages, E.hub_seq, hub_cells, st));
+  CK(cudaStreamSynchronize(st));
+  return ADDS_OK;
+}
+
+static int engine_upload_queries(Engine &E, cudaStream_t st) {
+  CK(cudaMemcpyAsync(E.qs, E.qs_host.data(), E.qs_host.size() * sizeof(QueryDesc),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return ADDS_OK;
+}
+
+/* Sizes the pool for the queries (x grow) and allocates everything. */
+static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQuery> &qv,
+                        unsigned grow, cudaStream_t st) {
+  engine_free(E);
+  E.device = device;
+  E.flt = flt;
+  E.nq = (unsigned)qv.size();
+  CK(adds_engine_prepare(flt, &E.max_bps, &E.block));
+  CK(cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device));
+  if (E.max_bps < 1 || E.num_sms < 1) return ADDS_ERR_UNSUPPORTED; /* kernel cannot be resident */
+  double sum_need = 0;
+  E.qs_host.resize(E.nq);
+  size_t pt_words = 0;
+  for (unsigned i = 0; i < E.nq; ++i) {
+    const EngQuery &q = qv[i];
+    const double need = 1.5 * q.n + q.m / 16.0 + 64.0;
+    sum_need += need;
+    unsigned ptl = next_pow2((unsigned long long)(need * grow / ADDS_PAGE) + 8ull);
+    if (ptl < 4) ptl = 4;
+    QueryDesc d;
+    memset(&d, 0, sizeof d);
+    d.row = q.row;
+    d.edges = q.edges;
+    d.dist = q.dist;
+    d.n = q.n;
+    d.src = q.src;
+    d.scale = q.scale;
+    d.ptn_log2 = ptl;
+    d.shift0 = q.shift;
+    d.graph_id = q.graph_id;
+    E.qs_host[i] = d;
+    pt_words += (size_t)ADDS_NB << ptl;
+    if (q.n > E.max_n) E.max_n = q.n;
+  }
+  unsigned long long pages = (unsigned long long)(sum_need * grow / ADDS_PAGE) + 2ull * ADDS_NB * E.nq + 64ull;
+  if (pages > 0x7FFFFFF0ull) return ADDS_ERR_OOM;
+  E.pool_pages = (unsigned)pages;
+  E.fq_cells = 1u << next_pow2(pages);
+  const unsigned hub_cells = 1u << ADDS_HUB_RING_LOG2;
+#define ALLOC(ptr, bytes_)                                          \
+  do {                                                              \
+    size_t _b = (bytes_);                                           \
+    cudaError_t _e = cudaMalloc((void **)&(ptr), _b);               \
+    if (_e != cudaSuccess) {                                        \
+      int _rc = cuda_fail(_e, "engine alloc " #ptr);                \
+      engine_free(E);                                               \
+      return _rc;                                                   \
+    }                                                               \
+    E.bytes += _b;                                                  \
+  } while (0)
+  ALLOC(E.pool, (size_t)E.pool_pages * ADDS_PAGE * 8);
+  ALLOC(E.pgen, (size_t)E.pool_pages * 4);
+  ALLOC(E.pcons, (size_t)E.pool_pages * 4);
+  ALLOC(E.fq, (size_t)E.fq_cells * 8);
+  ALLOC(E.hub, (size_t)hub_cells * sizeof(HubChunk));
+  ALLOC(E.hub_seq, (size_t)hub_cells * 4);
+  ALLOC(E.g, sizeof(GlobalCtl));
+  ALLOC(E.qs, (size_t)E.nq * sizeof(QueryDesc));
+  ALLOC(E.ctl, (size_t)E.nq * sizeof(QueryCtl));
+  ALLOC(E.slots, (size_t)E.nq * ADDS_NB * sizeof(SlotCtr));
+  ALLOC(E.pt, pt_words * 8);
+  ALLOC(E.reach, 16);
+#undef ALLOC
+  if (cudaMallocHost((void **)&E.g_host, sizeof(GlobalCtl)) != cudaSuccess) {
+    cudaGetLastError();
+    engine_free(E);
+    return ADDS_ERR_OOM;
+  }
+  size_t off = 0;
+  for (unsigned i = 0; i < E.nq; ++i) {
+    E.qs_host[i].pt = E.pt + off;
+    off += (size_t)ADDS_NB << E.qs_host[i].ptn_log2;
+    E.qs_host[i].slots = E.slots + (size_t)i * ADDS_NB;
+    E.qs_host[i].ctl = E.ctl + i;
+  }
+  int rc = engine_upload_queries(E, st);
+  if (rc) return rc;
+  return engine_full_reset(E, st);
+}
+
+/* resolved knobs */
+struct Knobs {
+  int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt;
+  unsigned long long timeout_ns;
+};
+
+static EngParams make_params(const Engine &E, const Knobs &k, unsigned single_src) {
+  EngParams P;
+  memset(&P, 0, sizeof P);
+  P.qs = E.qs;
+  P.nq = E.nq;
+  int cps = k.ctas_per_sm;
+  if (cps <= 0 || cps > E.max_bps) cps = E.max_bps;
+  P.nctas = (unsigned)(cps * E.num_sms);
+  P.g = E.g;
+  P.pool = E.pool;
+  P.pgen = E.pgen;
+  P.pcons = E.pcons;
+  P.fq = E.fq;
+  P.fq_mask = E.fq_cells - 1u;
+  P.pool_pages = E.pool_pages;
+  P.hub = E.hub;
+  P.hub_seq = E.hub_seq;
+  P.timeout_ns = k.timeout_ns;
+  P.alloc_wait_ns = 200ull * 1000ull * 1000ull;
+  if (P.alloc_wait_ns > k.timeout_ns) P.alloc_wait_ns = k.timeout_ns;
+  P.window = (unsigned)std::max(1, std::min(k.window, ADDS_NB));
+  P.batch_max = (unsigned)std::max(1, std::min(k.batch_max, E.block));
+  P.hub_threshold = (unsigned)std::max(k.hub_threshold, 64);
+  P.hub_chunk = (unsigned)std::max(k.hub_chunk, 64);
+  P.strict_order = (unsigned)k.strict;
+  P.adapt = (unsigned)k.adapt;
+  P.is_float = E.flt ? 1u : 0u;
+  P.single_src = single_src;
+  return P;
+}
+
+static int engine_enqueue(Engine &E, const EngParams &P, cudaStream_t st) {
+  CK(adds_engine_launch_init(P, E.max_n, st));
+  CK(adds_engine_launch_solve(P, st));
+  CK(cudaMemcpyAsync(E.g_host, E.g, sizeof(GlobalCtl), cudaMemcpyDeviceToHost, st));
+  return ADDS_OK;
+}
+
+/* device error word -> ABI code (after the stream has been synchronised) */
+static int engine_status(const Engine &E) {
+  switch (E.g_host->err) {
+    case ADDS_DEV_OK: return ADDS_OK;
+    case ADDS_DEV_OVERFLOW: return ADDS_ERR_WL_OVERFLOW;
+    case ADDS_DEV_HUB_OVERFLOW: return ADDS_ERR_WL_OVERFLOW;
+    default: return ADDS_ERR_DEVICE_TIMEOUT;
+  }
+}
+
+static void fill_stats(const Engine &E, const EngParams &P, adds_stats *s) {
+  if (!s) return;
+  const GlobalCtl &g = *E.g_host;
+  s->items_popped = g.st_items;
+  s->items_stale = g.st_stale;
+  s->edges_scanned = g.st_edges;
+  s->pushes = g.st_pushes;
+  s->batches = g.st_batches;
+  s->hub_chunks = g.st_hub;
+  s->ctas = (int32_t)P.nctas;
+}
+
+/* ------------------------------------------------------------------------ */
+/* graphs                                                                     */
+struct adds_graph {
+  int device = 0;
+  adds_wtype wt = ADDS_I32;
+  uint32_t n = 0;
+  uint64_t m = 0;
+  unsigned *row = nullptr;
+  uint2 *edges = nullptr;
+  unsigned *dist = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t max_deg = 0;
+  double avg_deg = 0, avg_w = 0;
+  size_t bytes = 0;
+  Engine eng;
+  unsigned grow = 1;
+  int tuned = 0;
+  adds_opts tuned_opts;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Knobs last_knobs;
+  EngParams last_params;
+  int pending = 0; /* async solves enqueued since the last sync */
+};
+
+static int set_device(int dev) {
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+    cudaGetLastError();
+    return ADDS_ERR_NO_DEVICE;
+  }
+  if (dev < 0 || dev >= cnt) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(dev));
+  return ADDS_OK;
+}
+
+static bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+/* graph validation + weight canonicalisation, on the device */
+__global__ void k_pack_edges(const uint32_t *dst, const uint32_t *w, uint64_t m, uint32_t n,
+                             int is_float, uint2 *edges, unsigned *bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = dst[i];
+    uint32_t x = w ? w[i] : 0u;
+    if (d >= n) atomicOr(bad, 1u);
+    if (is_float) {
+      if (x == 0x80000000u) x = 0u; /* -0.0 -> +0.0: identical sums */
+      if (x > 0x7F800000u) atomicOr(bad, 2u); /* negative or NaN */
+    } else if (x > 0x7FFFFFFFu) {
+      atomicOr(bad, 4u); /* negative as int32 */
+    }
+    edges[i] = make_uint2(d, x);
+  }
+}
+__global__ void k_set_weights(uint2 *edges, const uint32_t *w, uint64_t m, int is_float,
+                              unsigned *bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t x = w[i];
+    if (is_float) {
+      if (x == 0x80000000u) x = 0u;
+      if (x > 0x7F800000u) atomicOr(bad, 2u);
+    } else if (x > 0x7FFFFFFFu) {
+      atomicOr(bad, 4u);
+    }
+    edges[i].y = x;
+  }
+}
+__global__ void k_check_rows(const unsigned *row, uint32_t n, uint64_t m, unsigned *bad,
+                             unsigned *maxdeg) {
+  unsigned md = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const unsigned a = row[v], b = row[v + 1];
+    if (b < a || b > m) atomicOr(bad, 8u);
+    else md = max(md, b - a);
+  }
+  for (int o = 16; o > 0; o >>= 1) md = max(md, __shfl_down_sync(0xFFFFFFFFu, md, o));
+  if ((threadIdx.x & 31u) == 0u) atomicMax(maxdeg, md);
+}
+/* evenly spaced weight sample (profiler_kernel, ads_int/kernel.cu:153-183) */
+__global__ void k_sample_w(const uint2 *edges, uint64_t m, int is_float, unsigned ns, double *out) {
+  double acc = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+    const uint64_t e = (uint64_t)((double)i * (double)m / (double)ns);
+    const uint32_t x = edges[e < m ? e : m - 1].y;
+    acc += is_float ? (double)__uint_as_float(x) : (double)x;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31u) == 0u) atomicAdd(out, acc);
+}
+
+static int graph_finish(adds_graph *g) {
+  /* checks, degree/weight statistics, streams, result buffer */
+  unsigned *scratch = nullptr;
+  CK(cudaMalloc(&scratch, 64));
+  CK(cudaMemsetAsync(scratch, 0, 64, g->stream));
+  k_check_rows<<<592, 256, 0, g->stream>>>(g->row, g->n, g->m, scratch, scratch + 1);
+  const unsigned ns = (unsigned)std::min<uint64_t>(g->m, 1u << 16);
+  if (ns) k_sample_w<<<64, 256, 0, g->stream>>>(g->edges, g->m, g->wt == ADDS_F32, ns, (double *)(scratch + 2));
+  unsigned h[2];
+  double sw = 0;
+  CK(cudaMemcpyAsync(h, scratch, 8, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaMemcpyAsync(&sw, scratch + 2, 8, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(scratch);
+  if (h[0]) return ADDS_ERR_FORMAT;
+  g->max_deg = h[1];
+  g->avg_deg = g->n ? (double)g->m / g->n : 0.0;
+  g->avg_w = ns ? sw / ns : 1.0;
+  CK(cudaMalloc(&g->dist, ((size_t)g->n ? g->n : 1) * 4));
+  g->bytes += (size_t)g->n * 4;
+  CK(cudaEventCreate(&g->ev0));
+  CK(cudaEventCreate(&g->ev1));
+  return ADDS_OK;
+}
+
+static adds_graph *graph_new(int device, adds_wtype wt) {
+  adds_graph *g = new adds_graph();
+  g->device = device;
+  g->wt = wt;
+  adds_opts_init(&g->tuned_opts);
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete g;
+    return nullptr;
+  }
+  return g;
+}
+
+extern "C" void adds_graph_free(adds_graph *g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  engine_free(g->eng);
+  if (g->row) cudaFree(g->row);
+  if (g->edges) cudaFree(g->edges);
+  if (g->dist) cudaFree(g->dist);
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+/* Uploads dst/w (host or device) + u32 rows into g; validates on device. */
+static int graph_upload(adds_graph *g, const unsigned *row_host_u32, const uint32_t *dst,
+                        const void *w) {
+  const size_t m = g->m;
+  CK(cudaMalloc(&g->row, ((size_t)g->n + 1) * 4));
+  CK(cudaMalloc(&g->edges, (m ? m : 1) * sizeof(uint2)));
+  g->bytes = ((size_t)g->n + 1) * 4 + m * sizeof(uint2);
+  CK(cudaMemcpyAsync(g->row, row_host_u32, ((size_t)g->n + 1) * 4, cudaMemcpyHostToDevice, g->stream));
+  /* stream dst/w through device staging buffers in chunks */
+  const size_t CH = (size_t)1 << 26;
+  uint32_t *sd = nullptr, *sw = nullptr;
+  unsigned *bad = nullptr;
+  const size_t chunk = std::min(m ? m : 1, CH);
+  CK(cudaMalloc(&sd, chunk * 4));
+  CK(cudaMalloc(&sw, chunk * 4));
+  CK(cudaMalloc(&bad, 4));
+  CK(cudaMemsetAsync(bad, 0, 4, g->stream));
+  const bool dd = dst && is_device_ptr(dst), dw = w && is_device_ptr(w);
+  for (size_t off = 0; off < m; off += CH) {
+    const size_t c = std::min(CH, m - off);
+    CK(cudaMemcpyAsync(sd, dst + off, c * 4, dd ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, g->stream));
+    if (w)
+      CK(cudaMemcpyAsync(sw, (const uint32_t *)w + off, c * 4,
+                         dw ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, g->stream));
+    k_pack_edges<<<592, 256, 0, g->stream>>>(sd, w ? sw : nullptr, c, g->n, g->wt == ADDS_F32,
+                                             g->edges + off, bad);
+    /* the staging buffers are reused: wait before the next chunk */
+    CK(cudaStreamSynchronize(g->stream));
+  }
+  unsigned hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(sd);
+  cudaFree(sw);
+  cudaFree(bad);
+  if (hb & 1u) return ADDS_ERR_FORMAT;
+  if (hb & 6u) return ADDS_ERR_INVALID;
+  return graph_finish(g);
+}
+
+extern "C" int adds_graph_from_csr(uint32_t n, uint64_t m, const uint64_t *row_start,
+                                   const uint32_t *dst, const void *w, adds_wtype wt, int device,
+                                   adds_graph **out) {
+  if (!out || !row_start || (m && !dst) || n == 0 || n >= 0x80000000u || m >= 0xFFFFFFFFull ||
+      (wt != ADDS_I32 && wt != ADDS_F32))
+    return ADDS_ERR_INVALID;
+  *out = nullptr;
+  int rc = set_device(device);
+  if (rc) return rc;
+  if (row_start[0] != 0 || row_start[n] != m) return ADDS_ERR_INVALID;
+  std::vector<unsigned> row(n + 1);
+  for (uint32_t v = 0; v <= n; ++v) {
+    if (v && row_start[v] < row_start[v - 1]) return ADDS_ERR_INVALID;
+    row[v] = (unsigned)row_start[v];
+  }
+  adds_graph *g = graph_new(device, wt);
+  if (!g) return ADDS_ERR_CUDA;
+  g->n = n;
+  g->m = m;
+  rc = graph_upload(g, row.data(), dst, w);
+  if (rc) {
+    adds_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return ADDS_OK;
+}
+
+/* .gr v1 reader (readFromGR, ads_int/csr_graph.cu:203-296): mmap, check the
+ * header and the size, convert out_end[] to u32 row offsets, upload. */
+extern "C" int adds_graph_load_gr(const char *path, adds_wtype wt, int device, adds_graph **out) {
+  if (!path || !out || (wt != ADDS_I32 && wt != ADDS_F32)) return ADDS_ERR_INVALID;
+  *out = nullptr;
+  int rc = set_device(device);
+  if (rc) return rc;
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) return ADDS_ERR_IO;
+  struct stat sb;
+  if (fstat(fd, &sb) != 0) {
+    close(fd);
+    return ADDS_ERR_IO;
+  }
+  const size_t len = (size_t)sb.st_size;
+  if (len < 32) {
+    close(fd);
+    return ADDS_ERR_FORMAT;
+  }
+  void *map = mmap(nullptr, len, PROT_READ, MAP_PRIVATE, fd, 0);
+  close(fd);
+  if (map == MAP_FAILED) return ADDS_ERR_IO;
+  const uint64_t *h = (const uint64_t *)map;
+  const uint64_t version = h[0], esz = h[1], n64 = h[2], m64 = h[3];
+  rc = ADDS_OK;
+  adds_graph *g = nullptr;
+  std::vector<unsigned> row;
+  if (version != 1 || (esz != 0 && esz != 4) || n64 == 0 || n64 >= 0x80000000ull ||
+      m64 >= 0xFFFFFFFFull) {
+    rc = ADDS_ERR_FORMAT;
+  } else {
+    const size_t need = 32 + 8 * n64 + 4 * m64 + ((m64 & 1) ? 4 : 0) + (esz ? 4 * m64 : 0);
+    if (len < need) rc = ADDS_ERR_FORMAT;
+  }
+  if (!rc) {
+    const uint64_t *outidx = h + 4;
+    row.resize(n64 + 1);
+    row[0] = 0;
+    for (uint64_t v = 0; v < n64; ++v) {
+      const uint64_t e = outidx[v];
+      if (e < row[v] || e > m64) {
+        rc = ADDS_ERR_FORMAT;
+        break;
+      }
+      row[v + 1] = (unsigned)e;
+    }
+    if (!rc && row[n64] != m64) rc = ADDS_ERR_FORMAT;
+  }
+  if (!rc) {
+    const uint32_t *dst = (const uint32_t *)(h + 4 + n64);
+    const uint32_t *wv = esz ? dst + m64 + (m64 & 1) : nullptr;
+    g = graph_new(device, wt);
+    if (!g) rc = ADDS_ERR_CUDA;
+    else {
+      g->n = (uint32_t)n64;
+      g->m = m64;
+      rc = graph_upload(g, row.data(), dst, wv);
+    }
+  }
+  munmap(map, len);
+  if (rc) {
+    if (g) adds_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_generate(const adds_gen_spec *spec, int device, adds_graph **out) {
+  if (!spec || !out) return ADDS_ERR_INVALID;
+  *out = nullptr;
+  int rc = set_device(device);
+  if (rc) return rc;
+  adds_graph *g = graph_new(device, spec->wtype);
+  if (!g) return ADDS_ERR_CUDA;
+  uint32_t n = 0;
+  uint64_t m = 0;
+  rc = adds_gen_build(spec, &g->row, &g->edges, &n, &m, g->stream);
+  if (!rc) {
+    g->n = n;
+    g->m = m;
+    g->bytes = ((size_t)n + 1) * 4 + m * sizeof(uint2);
+    rc = graph_finish(g);
+  }
+  if (rc) {
+    adds_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_info(const adds_graph *g, adds_graph_info_t *info) {
+  if (!g || !info) return ADDS_ERR_INVALID;
+  info->n = g->n;
+  info->m = g->m;
+  info->wtype = g->wt;
+  info->device = g->device;
+  info->max_degree = g->max_deg;
+  info->avg_degree = g->avg_deg;
+  info->avg_weight = g->avg_w;
+  info->device_bytes = g->bytes + g->eng.bytes;
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_download(const adds_graph *g, uint64_t *row_start, uint32_t *dst, void *w) {
+  if (!g) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(g->device));
+  if (row_start) {
+    std::vector<unsigned> r(g->n + 1);
+    CK(cudaMemcpy(r.data(), g->row, ((size_t)g->n + 1) * 4, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i <= g->n; ++i) row_start[i] = r[i];
+  }
+  if (dst || w) {
+    const size_t CH = (size_t)1 << 24;
+    std::vector<uint2> buf(std::min<size_t>(g->m ? g->m : 1, CH));
+    for (size_t off = 0; off < g->m; off += CH) {
+      const size_t c = std::min(CH, (size_t)g->m - off);
+      CK(cudaMemcpy(buf.data(), g->edges + off, c * sizeof(uint2), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < c; ++i) {
+        if (dst) dst[off + i] = buf[i].x;
+        if (w) ((uint32_t *)w)[off + i] = buf[i].y;
+      }
+    }
+  }
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_set_weights(adds_graph *g, const void *w) {
+  if (!g || !w) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(g->device));
+  if (g->m == 0) return ADDS_OK;
+  const uint32_t *src = (const uint32_t *)w;
+  uint32_t *tmp = nullptr;
+  if (!is_device_ptr(w)) {
+    CK(cudaMalloc(&tmp, g->m * 4));
+    CK(cudaMemcpyAsync(tmp, w, g->m * 4, cudaMemcpyHostToDevice, g->stream));
+    src = tmp;
+  }
+  unsigned *bad = nullptr;
+  CK(cudaMalloc(&bad, 4));
+  CK(cudaMemsetAsync(bad, 0, 4, g->stream));
+  k_set_weights<<<592, 256, 0, g->stream>>>(g->edges, src, g->m, g->wt == ADDS_F32, bad);
+  unsigned hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  if (tmp) cudaFree(tmp);
+  cudaFree(bad);
+  if (hb) return ADDS_ERR_INVALID;
+  /* the weight sample feeds the automatic delta */
+  double sw = 0;
+  double *d_sw = nullptr;
+  CK(cudaMalloc(&d_sw, 8));
+  CK(cudaMemsetAsync(d_sw, 0, 8, g->stream));
+  const unsigned ns = (unsigned)std::min<uint64_t>(g->m, 1u << 16);
+  k_sample_w<<<64, 256, 0, g->stream>>>(g->edges, g->m, g->wt == ADDS_F32, ns, d_sw);
+  CK(cudaMemcpyAsync(&sw, d_sw, 8, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(d_sw);
+  g->avg_w = sw / ns;
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_save_gr(const adds_graph *g, const char *path) {
+  if (!g || !path) return ADDS_ERR_INVALID;
+  std::vector<uint64_t> row(g->n + 1);
+  std::vector<uint32_t> dst(g->m), w(g->m);
+  int rc = adds_graph_download(g, row.data(), dst.data(), w.data());
+  if (rc) return rc;
+  FILE *f = fopen(path, "wb");
+  if (!f) return ADDS_ERR_IO;
+  const uint64_t hdr[4] = {1, 4, g->n, g->m};
+  bool ok = fwrite(hdr, 8, 4, f) == 4;
+  ok = ok && fwrite(row.data() + 1, 8, g->n, f) == g->n;
+  ok = ok && fwrite(dst.data(), 4, g->m, f) == g->m;
+  if (g->m & 1) {
+    const uint32_t pad = 0;
+    ok = ok && fwrite(&pad, 4, 1, f) == 1;
+  }
+  ok = ok && fwrite(w.data(), 4, g->m, f) == g->m;
+  if (fclose(f) != 0) ok = false;
+  return ok ? ADDS_OK : ADDS_ERR_IO;
+}
+
+/* ------------------------------------------------------------------------ */
+/* knob resolution: explicit opts > tuned values > degree/weight heuristic   */
+static float auto_scale(const adds_graph *g) {
+  const double aw = g->avg_w > 1e-30 ? g->avg_w : 1.0;
+  return (float)(65536.0 / aw); /* 1 key unit = avg_w / 2^16 */
+}
+
+/* Delta ~ 8 * avg_weight / avg_degree (the reference starts from
+ * avg_wt/avg_degree/32 and raises it on the device, wl.h:414-440, 968-1360;
+ * on 148 SMs a wider bucket is the better starting point). */
+static int auto_shift(const adds_graph *g) {
+  const double deg = g->avg_deg > 1.0 ? g->avg_deg : 1.0;
+  double delta_keys;
+  if (g->wt == ADDS_F32) delta_keys = 8.0 * 65536.0 / deg;
+  else delta_keys = 8.0 * (g->avg_w > 1.0 ? g->avg_w : 1.0) / deg;
+  int s = (int)lround(log2(delta_keys > 1.0 ? delta_keys : 1.0));
+  return std::max(0, std::min(s, 31));
+}
+
+static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shift, float *scale) {
+  adds_opts d;
+  adds_opts_init(&d);
+  const adds_opts *t = g->tuned ? &g->tuned_opts : &d;
+  if (!o) o = &d;
+  *shift = o->delta_shift >= 0 ? o->delta_shift : (t->delta_shift >= 0 ? t->delta_shift : auto_shift(g));
+  *scale = o->delta_scale > 0 ? o->delta_scale : (t->delta_scale > 0 ? t->delta_scale : auto_scale(g));
+  k->window = o->window > 0 ? o->window : (t->window > 0 ? t->window : 2);
+  k->ctas_per_sm = o->ctas_per_sm > 0 ? o->ctas_per_sm : t->ctas_per_sm;
+  k->batch_max = o->batch_max > 0 ? o->batch_max : (t->batch_max > 0 ? t->batch_max : 512);
+  k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : 16384);
+  k->hub_chunk = 4096;
+  k->strict = o->strict_order >= 0 ? o->strict_order : (t->strict_order >= 0 ? t->strict_order : 1);
+  k->adapt = o->adapt >= 0 ? o->adapt : (t->adapt >= 0 ? t->adapt : 0);
+  const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
+  k->timeout_ns = (unsigned long long)tmo * 1000000ull;
+}
+
+/* ------------------------------------------------------------------------ */
+/* plain solves                                                               */
+static int graph_engine(adds_graph *g, int shift, float scale) {
+  if (g->eng.nq == 1 && g->eng.qs_host[0].shift0 == (unsigned)shift && g->eng.qs_host[0].scale == scale)
+    return ADDS_OK;
+  if (g->eng.nq == 1) { /* same sizing: only the descriptor changes */
+    g->eng.qs_host[0].shift0 = (unsigned)shift;
+    g->eng.qs_host[0].scale = scale;
+    return engine_upload_queries(g->eng, g->stream);
+  }
+  std::vector<EngQuery> qv(1);
+  qv[0] = EngQuery{g->row, g->edges, g->dist, g->n, g->m, 0u, scale, (unsigned)shift, 0u};
+  return engine_alloc(g->eng, g->device, g->wt == ADDS_F32, qv, g->grow, g->stream);
+}
+
+static cudaStream_t pick_stream(const adds_graph *g, const adds_opts *o) {
+  return (o && o->stream) ? (cudaStream_t)o->stream : g->stream;
+}
+
+/* Enqueues one solve; no host synchronisation. */
+static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts, bool timed) {
+  int shift;
+  float scale;
+  Knobs k;
+  resolve(g, opts, &k, &shift, &scale);
+  int rc = graph_engine(g, shift, scale);
+  if (rc) return rc;
+  cudaStream_t st = pick_stream(g, opts);
+  EngParams P = make_params(g->eng, k, src);
+  g->last_knobs = k;
+  g->last_params = P;
+  if (timed) CK(cudaEventRecord(g->ev0, st));
+  rc = engine_enqueue(g->eng, P, st);
+  if (rc) return rc;
+  if (timed) CK(cudaEventRecord(g->ev1, st));
+  return ADDS_OK;
+}
+
+extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds_opts *opts,
+                         adds_stats *stats) {
+  if (!g || src >= g->n) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  cudaStream_t st = pick_stream(g, opts);
+  int retries = 0;
+  for (;;) {
+    rc = sssp_enqueue(g, src, opts, true);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    rc = engine_status(g->eng);
+    if (rc == ADDS_ERR_WL_OVERFLOW && retries < 4) {
+      ++retries;
+      g->grow *= 2;
+      g->eng.nq = 0; /* force re-allocation at the larger size */
+      engine_free(g->eng);
+      continue;
+    }
+    if (rc) {
+      engine_full_reset(g->eng, st);
+      return rc;
+    }
+    break;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    stats->ms = ms;
+    fill_stats(g->eng, g->last_params, stats);
+    stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+    stats->retries = retries;
+  }
+  g->pending = 0;
+  if (dist_out) return adds_graph_last_dist(g, dist_out);
+  return ADDS_OK;
+}
+
+/* Asynchronous form for back-to-back solves: errors surface in
+ * adds_graph_sync (a failed solve makes the following ones exit at once). */
+extern "C" int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opts) {
+  if (!g || src >= g->n) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  rc = sssp_enqueue(g, src, opts, false);
+  if (!rc) ++g->pending;
+  return rc;
+}
+
+extern "C" int adds_graph_sync(adds_graph *g, adds_stats *stats) {
+  if (!g) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(g->stream));
+  if (g->eng.nq == 0) return ADDS_OK;
+  rc = engine_status(g->eng);
+  g->pending = 0;
+  if (rc) {
+    engine_full_reset(g->eng, g->stream);
+    return rc;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    fill_stats(g->eng, g->last_params, stats);
+    stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+  }
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_last_dist(adds_graph *g, void *dist_out) {
+  if (!g || !dist_out) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(g->device));
+  const bool dev = is_device_ptr(dist_out);
+  CK(cudaMemcpyAsync(dist_out, g->dist, (size_t)g->n * 4,
+                     dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_reached(adds_graph *g, uint64_t *reached, uint64_t *reached_edges) {
+  if (!g) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(g->device));
+  unsigned long long *d = nullptr, h[2] = {0, 0};
+  CK(cudaMalloc(&d, 16));
+  CK(cudaMemsetAsync(d, 0, 16, g->stream));
+  CK(adds_engine_launch_reached(g->row, g->dist, g->n,
+                                g->wt == ADDS_F32 ? ADDS_INF_F32_BITSV : ADDS_INF_I32_BITS, d,
+                                g->stream));
+  CK(cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(d);
+  if (reached) *reached = h[0];
+  if (reached_edges) *reached_edges = h[1];
+  return ADDS_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* batches                                                                    */
+struct adds_batch {
+  int device = 0;
+  bool flt = false;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<adds_graph *> qgraph;
+  std::vector<uint32_t> srcs;
+  std::vector<adds_graph *> ugraph; /* distinct graphs, first-use order */
+  std::vector<unsigned> qgid;
+  unsigned *dist_all = nullptr;
+  std::vector<size_t> dist_off;
+  Engine eng;
+  unsigned grow = 1;
+  Knobs kn;
+  std::vector<int> shifts;
+  std::vector<float> scales;
+  cudaGraphExec_t exec = nullptr;
+  bool captured = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  EngParams P;
+  void *adj = nullptr; /* backward scratch (adjoint.cu) */
+};
+
+static int batch_engine(adds_batch *b) {
+  std::vector<EngQuery> qv(b->qgraph.size());
+  for (size_t i = 0; i < qv.size(); ++i) {
+    adds_graph *g = b->qgraph[i];
+    qv[i] = EngQuery{g->row, g->edges, b->dist_all + b->dist_off[i], g->n, g->m, b->srcs[i],
+                     b->scales[i], (unsigned)b->shifts[i], b->qgid[i]};
+  }
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  b->captured = false;
+  int rc = engine_alloc(b->eng, b->device, b->flt, qv, b->grow, b->stream);
+  if (rc) return rc;
+  b->P = make_params(b->eng, b->kn, 0xFFFFFFFFu);
+  return ADDS_OK;
+}
+
+extern "C" void adds_batch_free(adds_batch *b);
+void adds_adjoint_free(void *adj);
+
+extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs, uint32_t nq,
+                                 const adds_opts *opts, adds_batch **out) {
+  if (!graphs || !srcs || !out || nq == 0 || nq > 65535) return ADDS_ERR_INVALID;
+  *out = nullptr;
+  const int dev = graphs[0]->device;
+  const adds_wtype wt = graphs[0]->wt;
+  for (uint32_t i = 0; i < nq; ++i) {
+    if (!graphs[i] || graphs[i]->device != dev || graphs[i]->wt != wt || srcs[i] >= graphs[i]->n)
+      return ADDS_ERR_INVALID;
+  }
+  int rc = set_device(dev);
+  if (rc) return rc;
+  adds_batch *b = new adds_batch();
+  b->device = dev;
+  b->flt = wt == ADDS_F32;
+  if (opts && opts->stream) b->stream = (cudaStream_t)opts->stream;
+  else {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      delete b;
+      return ADDS_ERR_CUDA;
+    }
+    b->own_stream = true;
+  }
+  b->qgraph.assign(graphs, graphs + nq);
+  b->srcs.assign(srcs, srcs + nq);
+  size_t tot = 0;
+  b->dist_off.resize(nq);
+  b->shifts.resize(nq);
+  b->scales.resize(nq);
+  for (uint32_t i = 0; i < nq; ++i) {
+    adds_graph *g = graphs[i];
+    auto it = std::find(b->ugraph.begin(), b->ugraph.end(), g);
+    unsigned gid = (unsigned)(it - b->ugraph.begin());
+    if (it == b->ugraph.end()) b->ugraph.push_back(g);
+    b->qgid.push_back(gid);
+    b->dist_off[i] = tot;
+    tot += ((size_t)g->n + 31) & ~(size_t)31;
+    Knobs k;
+    resolve(g, opts, &k, &b->shifts[i], &b->scales[i]);
+    if (i == 0) b->kn = k;
+  }
+  if (cudaMalloc(&b->dist_all, tot * 4) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    adds_batch_free(b);
+    return ADDS_ERR_OOM;
+  }
+  rc = batch_engine(b);
+  if (rc) {
+    adds_batch_free(b);
+    return rc;
+  }
+  *out = b;
+  return ADDS_OK;
+}
+
+extern "C" void adds_batch_free(adds_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  engine_free(b->eng);
+  if (b->dist_all) cudaFree(b->dist_all);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->adj) adds_adjoint_free(b->adj);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+/* init + solve + status read-back, captured once as a CUDA graph */
+static int batch_capture(adds_batch *b) {
+  cudaGraph_t gr = nullptr;
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = engine_enqueue(b->eng, b->P, b->stream);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+  if (rc || e != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    cudaGetLastError();
+    return rc ? rc : cuda_fail(e, "capture");
+  }
+  e = cudaGraphInstantiate(&b->exec, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return cuda_fail(e, "instantiate");
+  b->captured = true;
+  return ADDS_OK;
+}
+
+extern "C" int adds_batch_launch(adds_batch *b) {
+  if (!b) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(b->device));
+  if (!b->captured) {
+    int rc = batch_capture(b);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(b->ev0, b->stream));
+  CK(cudaGraphLaunch(b->exec, b->stream));
+  CK(cudaEventRecord(b->ev1, b->stream));
+  return ADDS_OK;
+}
+
+extern "C" int adds_batch_sync(adds_batch *b, adds_stats *stats) {
+  if (!b) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  int rc = engine_status(b->eng);
+  if (rc) return rc;
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    stats->ms = ms;
+    fill_stats(b->eng, b->P, stats);
+    stats->delta_shift = b->shifts.empty() ? 0 : b->shifts[0];
+  }
+  return ADDS_OK;
+}
+
+extern "C" int adds_batch_run(adds_batch *b, adds_stats *stats) {
+  if (!b) return ADDS_ERR_INVALID;
+  int retries = 0;
+  for (;;) {
+    int rc = adds_batch_launch(b);
+    if (rc) return rc;
+    rc = adds_batch_sync(b, stats);
+    if (rc == ADDS_ERR_WL_OVERFLOW && retries < 4) {
+      ++retries;
+      b->grow *= 2;
+      rc = batch_engine(b);
+      if (rc) return rc;
+      continue;
+    }
+    if (rc) {
+      engine_full_reset(b->eng, b->stream);
+      return rc;
+    }
+    if (stats) stats->retries = retries;
+    return ADDS_OK;
+  }
+}
+
+extern "C" int adds_batch_set_sources(adds_batch *b, const uint32_t *srcs) {
+  if (!b || !srcs) return ADDS_ERR_INVALID;
+  for (size_t i = 0; i < b->srcs.size(); ++i)
+    if (srcs[i] >= b->qgraph[i]->n) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (size_t i = 0; i < b->srcs.size(); ++i) {
+    b->srcs[i] = srcs[i];
+    b->eng.qs_host[i].src = srcs[i];
+  }
+  return engine_upload_queries(b->eng, b->stream);
+}
+
+extern "C" int adds_batch_dist_ptr(adds_batch *b, uint32_t q, void **dptr) {
+  if (!b || !dptr || q >= b->srcs.size()) return ADDS_ERR_INVALID;
+  *dptr = b->dist_all + b->dist_off[q];
+  return ADDS_OK;
+}
+
+extern "C" int adds_batch_dist(adds_batch *b, uint32_t q, void *out) {
+  if (!b || !out || q >= b->srcs.size()) return ADDS_ERR_INVALID;
+  CK(cudaSetDevice(b->device));
+  const bool dev = is_device_ptr(out);
+  CK(cudaMemcpyAsync(out, b->dist_all + b->dist_off[q], (size_t)b->qgraph[q]->n * 4,
+                     dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return ADDS_OK;
+}
+
+/* accessors used by adjoint.cu */
+int adds_batch_internal(adds_batch *b, cudaStream_t *st, unsigned *nq,
+                        std::vector<adds_graph *> **qgraph, std::vector<uint32_t> **srcs,
+                        std::vector<adds_graph *> **ugraph, std::vector<unsigned> **qgid,
+                        unsigned **dist_all, std::vector<size_t> **dist_off, void ***adj) {
+  *st = b->stream;
+  *nq = (unsigned)b->srcs.size();
+  *qgraph = &b->qgraph;
+  *srcs = &b->srcs;
+  *ugraph = &b->ugraph;
+  *qgid = &b->qgid;
+  *dist_all = b->dist_all;
+  *dist_off = &b->dist_off;
+  *adj = &b->adj;
+  return ADDS_OK;
+}
+void adds_graph_internal(const adds_graph *g, const unsigned **row, const uint2 **edges,
+                         uint32_t *n, uint64_t *m, int *device) {
+  *row = g->row;
+  *edges = g->edges;
+  *n = g->n;
+  *m = g->m;
+  *device = g->device;
+}
+
+/* ------------------------------------------------------------------------ */
+/* autotuner: coordinate descent over (delta, window, batch, CTAs/SM, hub
+ * threshold) on the sample sources; stores the winner in the graph. */
+static double time_solves(adds_graph *g, const uint32_t *srcs, uint32_t ns, const adds_opts *o) {
+  for (uint32_t i = 0; i < ns; ++i)
+    if (adds_sssp_async(g, srcs[i], o)) return 1e30; /* warm */
+  if (adds_graph_sync(g, nullptr)) return 1e30;
+  cudaEvent_t a, z;
+  cudaEventCreate(&a);
+  cudaEventCreate(&z);
+  cudaEventRecord(a, g->stream);
+  for (uint32_t i = 0; i < ns; ++i)
+    if (adds_sssp_async(g, srcs[i], o)) {
+      cudaEventDestroy(a);
+      cudaEventDestroy(z);
+      return 1e30;
+    }
+  cudaEventRecord(z, g->stream);
+  const int rc = adds_graph_sync(g, nullptr);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, z);
+  cudaEventDestroy(a);
+  cudaEventDestroy(z);
+  return rc ? 1e30 : (double)ms;
+}
+
+extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_opts *best,
+                         double *best_ms) {
+  if (!g || !srcs || ns == 0) return ADDS_ERR_INVALID;
+  for (uint32_t i = 0; i < ns; ++i)
+    if (srcs[i] >= g->n) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  g->tuned = 0;
+  adds_opts cur;
+  adds_opts_init(&cur);
+  Knobs k;
+  int s0;
+  float sc;
+  resolve(g, &cur, &k, &s0, &sc);
+  cur.delta_shift = s0;
+  cur.delta_scale = sc;
+  cur.window = k.window;
+  cur.batch_max = k.batch_max;
+  cur.hub_threshold = k.hub_threshold;
+  cur.strict_order = k.strict;
+  double bm = time_solves(g, srcs, ns, &cur);
+  auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
+    for (int v : vals) {
+      if (v == cur.*f) continue;
+      adds_opts t = cur;
+      t.*f = v;
+      const double ms = time_solves(g, srcs, ns, &t);
+      if (ms < bm * 0.98) {
+        bm = ms;
+        cur = t;
+      }
+    }
+  };
+  std::vector<int> shifts;
+  for (int d = -4; d <= 4; ++d)
+    if (s0 + d >= 0 && s0 + d <= 31) shifts.push_back(s0 + d);
+  try_field(&adds_opts::delta_shift, shifts);
+  try_field(&adds_opts::window, {1, 2, 3, 4, 8});
+  try_field(&adds_opts::batch_max, {64, 128, 256, 512});
+  try_field(&adds_opts::hub_threshold, {2048, 4096, 16384, 65536});
+  int maxb = g->eng.max_bps;
+  std::vector<int> cps;
+  for (int c = 1; c <= maxb; ++c) cps.push_back(c);
+  try_field(&adds_opts::ctas_per_sm, cps);
+  try_field(&adds_opts::strict_order, {0, 1});
+  if (cur.delta_shift != s0) { /* second look around the new delta */
+    std::vector<int> s2;
+    for (int d = -1; d <= 1; ++d)
+      if (cur.delta_shift + d >= 0 && cur.delta_shift + d <= 31) s2.push_back(cur.delta_shift + d);
+    try_field(&adds_opts::delta_shift, s2);
+  }
+  if (bm >= 1e29) return ADDS_ERR_DEVICE_TIMEOUT;
+  g->tuned_opts = cur;
+  g->tuned_opts.stream = nullptr;
+  g->tuned = 1;
+  if (best) *best = g->tuned_opts;
+  if (best_ms) *best_ms = bm / ns;
+  return ADDS_OK;
+}

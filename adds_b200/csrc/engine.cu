@@ -1,0 +1,808 @@
+/*
+ * engine.cu — persistent asynchronous delta-stepping SSSP for sm_100a.
+ *
+ * Behavioural source: ADDS (ads_int/kernel.cu:30-128 workers,
+ * ads_int/wl.h:192-1972 worklist + manager).  What is kept:
+ *   - 32 circular distance buckets per solve, bucket = clip(dist >> shift
+ *     relative to the lowest live bucket, 0, 31) (wl.h:1958-1972);
+ *   - several consecutive buckets may be processed at once (the reference's
+ *     concur_bag, wl.h:1398-1510), the lowest is retired only once it is
+ *     empty and none of its entries is still being processed (wl.h:714-724);
+ *   - relax = new = d[u] + w, accept if d[v] > new, atomicMin, push
+ *     (kernel.cu:112-121); float uses the IEEE bit order of non-negative
+ *     floats for the 32-bit atomicMin instead of the reference's 64-bit CAS
+ *     (ads_float/csr_graph.h:58-70); rows longer than a threshold are split
+ *     across workers (wl.h:1638-1696, here across the whole grid).
+ * What is new: no manager block and no CDP.  One cooperative launch of
+ * CTAs that pop whole batches from the bucket queues with a CAS, expand the
+ * batch edge-balanced over the CTA, stage pushes in shared memory and flush
+ * them with one reservation per bucket.  Queue entries are (vertex, pushed
+ * distance) pairs; an entry whose vertex has since improved is dropped.
+ * Termination is a per-query count of live entries.  Every wait is bounded
+ * by a device deadline and reports ADDS_DEV_TIMEOUT instead of hanging.
+ */
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "adds_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace adds {
+
+/* ------------------------------------------------------------------------ */
+/* memory-model helpers (PTX ISA: ld/st .relaxed.gpu, globaltimer)           */
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned long long ld_rlx64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_rlx32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acq32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_rlx64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_rlx32(unsigned *p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+/* where a wait gave up (GlobalCtl::err_where) */
+enum : unsigned {
+  W_ALLOC = 1, W_PT = 2, W_ENTRY = 3, W_HUB_PUB = 4, W_HUB_POP = 5, W_IDLE = 6,
+  W_SPAN = 7, W_INIT = 8
+};
+
+__device__ __forceinline__ void raise_err(GlobalCtl *g, unsigned code, unsigned where) {
+  if (atomicCAS(&g->err, 0u, code) == 0u) st_rlx32(&g->err_where, where);
+}
+
+/* Bounded wait: call once per spin iteration; false = give up. */
+struct Waiter {
+  unsigned long long deadline;
+  unsigned it;
+  unsigned code; /* error raised when the deadline passes */
+  __device__ __forceinline__ bool spin(GlobalCtl *g, unsigned where) {
+    ++it;
+    if ((it & 15u) == 0u) {
+      if (ld_rlx32(&g->err) != 0u) return false;
+      if (gtimer() > deadline) {
+        raise_err(g, code, where);
+        return false;
+      }
+    }
+    __nanosleep(it < 64 ? 20 : 200);
+    return true;
+  }
+};
+
+#define PAGE_MASK (ADDS_PAGE - 1u)
+#define PI_BAD 0xFFFFFFFFu /* page-info sentinel: phys | phase << 31 */
+
+/* ------------------------------------------------------------------------ */
+/* page pool                                                                  */
+
+/* Pops a free page (MPMC ticket queue).  Replaces alloc_manager
+ * (wl.h:488-622), which pre-mapped pages ahead of each bag from one warp. */
+__device__ unsigned alloc_page(const EngParams &P, unsigned long long deadline) {
+  GlobalCtl *g = P.g;
+  const unsigned long long t = atomicAdd(&g->fq_head, 1ull);
+  unsigned long long *cell = &P.fq[t & P.fq_mask];
+  const unsigned long long give_up = gtimer() + P.alloc_wait_ns;
+  /* no page back within alloc_wait_ns means the pool is exhausted */
+  Waiter w{deadline < give_up ? deadline : give_up, 0,
+           deadline < give_up ? (unsigned)ADDS_DEV_TIMEOUT : (unsigned)ADDS_DEV_OVERFLOW};
+  for (;;) {
+    const unsigned long long e = ld_rlx64(cell);
+    if ((unsigned)e == (unsigned)t) {
+      const unsigned phys = (unsigned)(e >> 32);
+      const unsigned gen = atomicAdd(&P.pgen[phys], 1u) + 1u;
+      return phys | ((gen & 1u) << 31);
+    }
+    if (!w.spin(g, W_ALLOC)) return PI_BAD;
+  }
+}
+
+__device__ void free_page(const EngParams &P, unsigned phys) {
+  atomicExch(&P.pcons[phys], 0u);
+  __threadfence();
+  const unsigned long long t = atomicAdd(&P.g->fq_tail, 1ull);
+  st_rlx64(&P.fq[t & P.fq_mask], ((unsigned long long)phys << 32) | (unsigned)t);
+}
+
+/* Marks cnt entries of page pi consumed; frees the page when all are. */
+__device__ __forceinline__ void consume(const EngParams &P, unsigned pi, unsigned cnt) {
+  if (pi == PI_BAD || cnt == 0) return;
+  const unsigned phys = pi & 0x7FFFFFFFu;
+  const unsigned old = atomicAdd(&P.pcons[phys], cnt);
+  if (old + cnt == ADDS_PAGE) free_page(P, phys);
+}
+
+__device__ __forceinline__ unsigned long long *pt_cell(const QueryDesc &d, unsigned s,
+                                                       unsigned long long vp) {
+  return d.pt + (((unsigned long long)s << d.ptn_log2) |
+                 (vp & ((1ull << d.ptn_log2) - 1ull)));
+}
+
+/* Waits until virtual page vp of slot s is mapped (translate_write_ptr,
+ * wl.h:1874-1900, resolved from an HBM page table instead of a smem cache). */
+__device__ unsigned pt_wait(const EngParams &P, const QueryDesc &d, unsigned s,
+                            unsigned long long vp, unsigned long long deadline) {
+  unsigned long long *cell = pt_cell(d, s, vp);
+  Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
+  for (;;) {
+    const unsigned long long e = ld_rlx64(cell);
+    if ((unsigned)e == (unsigned)vp) return (unsigned)(e >> 32);
+    if (!w.spin(P.g, W_PT)) return PI_BAD;
+  }
+}
+
+/* Reserves c entries at the tail of slot s; maps the (at most two) pages the
+ * range touches.  The reservation that contains a page's first entry
+ * allocates it; others wait for the mapping.  Replaces push_work's
+ * reservation + translate (wl.h:1902-1928). */
+__device__ bool slot_reserve(const EngParams &P, const QueryDesc &d, unsigned s,
+                             unsigned c, unsigned long long deadline,
+                             unsigned long long *pbase, unsigned *pp0, unsigned *pp1) {
+  SlotCtr *sc = d.slots + s;
+  const unsigned long long base = atomicAdd(&sc->tail, (unsigned long long)c);
+  *pbase = base;
+  *pp0 = *pp1 = PI_BAD;
+  const unsigned long long head = ld_rlx64(&sc->head);
+  const unsigned long long ptn = 1ull << d.ptn_log2;
+  if (base + c - head > (ptn - 3ull) * ADDS_PAGE) {
+    raise_err(P.g, ADDS_DEV_OVERFLOW, W_SPAN);
+    return false;
+  }
+  const unsigned long long vp0 = base >> ADDS_PAGE_LOG2;
+  const unsigned long long vp1 = (base + c - 1) >> ADDS_PAGE_LOG2;
+  for (unsigned long long vp = vp0; vp <= vp1; ++vp) {
+    unsigned pi;
+    if ((vp << ADDS_PAGE_LOG2) >= base) {
+      pi = alloc_page(P, deadline);
+      if (pi == PI_BAD) return false;
+      st_rlx64(pt_cell(d, s, vp), ((unsigned long long)pi << 32) | (unsigned)vp);
+    } else {
+      pi = pt_wait(P, d, s, vp, deadline);
+      if (pi == PI_BAD) return false;
+    }
+    if (vp == vp0) *pp0 = pi; else *pp1 = pi;
+  }
+  if (vp1 == vp0) *pp1 = *pp0;
+  return true;
+}
+
+__device__ __forceinline__ unsigned long long *entry_ptr(const EngParams &P, unsigned pi,
+                                                         unsigned long long idx) {
+  return P.pool + ((((unsigned long long)(pi & 0x7FFFFFFFu)) << ADDS_PAGE_LOG2) |
+                   (idx & PAGE_MASK));
+}
+__device__ __forceinline__ unsigned long long make_entry(unsigned v, unsigned d,
+                                                         unsigned pi) {
+  return ((unsigned long long)d << 32) | (v & 0x7FFFFFFFu) | (pi & 0x80000000u);
+}
+
+/* ------------------------------------------------------------------------ */
+/* bucket mapping (dist_to_bag_id_int, wl.h:1958-1972)                        */
+template <bool FLT>
+__device__ __forceinline__ unsigned dist_key(unsigned d, float scale) {
+  if (FLT) return __float2uint_rz(__fmul_rn(__uint_as_float(d), scale));
+  return d;
+}
+__device__ __forceinline__ unsigned bucket_slot(unsigned key, unsigned shift,
+                                                unsigned base_b, unsigned base_key) {
+  const unsigned kk = key >> shift;
+  const unsigned off = kk > base_key ? min(kk - base_key, (unsigned)ADDS_NB - 1u) : 0u;
+  return (base_b + off) & (ADDS_NB - 1u);
+}
+
+/* ------------------------------------------------------------------------ */
+/* shared memory of one CTA                                                   */
+template <int BLOCK>
+struct Smem {
+  static constexpr int U = 4;               /* edges per thread per round    */
+  static constexpr int SB = 2 * BLOCK * U;  /* staged pushes                 */
+  unsigned it_rb[BLOCK];                    /* first edge of each item       */
+  unsigned it_du[BLOCK];                    /* distance used for the item    */
+  unsigned it_off[BLOCK];                   /* exclusive scan of degrees     */
+  unsigned pb_v[SB];
+  unsigned pb_d[SB];
+  unsigned short pb_rank[SB];
+  unsigned char pb_s[SB];
+  unsigned long long bbase[ADDS_NB];
+  unsigned bp0[ADDS_NB];
+  unsigned bp1[ADDS_NB];
+  unsigned hist[ADDS_NB];
+  unsigned wsum[BLOCK / 32];
+  /* batch descriptor written by the acquiring warp */
+  unsigned long long h;
+  unsigned status, q, slot, k;
+  unsigned pi0, pi1;
+  unsigned base_b, base_key, shift;
+  unsigned pcnt, total_edges, hub_chunks;
+  unsigned cur_q, idle;
+};
+
+enum : unsigned { ST_WORK = 0, ST_HUB = 1, ST_IDLE = 2, ST_EXIT = 3 };
+
+/* ------------------------------------------------------------------------ */
+/* Acquire a batch (warp 0).  Replaces the assign manager + get_global
+ * mailbox handshake (wl.h:851-1527, 1698-1853): the CTA itself pops from
+ * the lowest non-empty bucket in the window with a CAS on the slot head and
+ * retires the lowest bucket when it is empty and drained. */
+template <int BLOCK>
+__device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
+                        unsigned long long deadline) {
+  const unsigned lane = threadIdx.x & 31u;
+  GlobalCtl *g = P.g;
+  if (ld_rlx32(&g->err) != 0u || ld_rlx32(&g->remaining) == 0u) {
+    if (lane == 0) S.status = ST_EXIT;
+    return;
+  }
+  /* 1. split-row chunks first: they belong to vertices already popped */
+  {
+    unsigned long long ticket = ~0ull;
+    if (lane == 0) {
+      unsigned long long hh = ld_rlx64(&g->hub_head);
+      for (int tries = 0; tries < 4; ++tries) {
+        const unsigned long long ht = ld_rlx64(&g->hub_tail);
+        if (hh >= ht) break;
+        const unsigned long long prev = atomicCAS(&g->hub_head, hh, hh + 1ull);
+        if (prev == hh) { ticket = hh; break; }
+        hh = prev;
+      }
+    }
+    ticket = __shfl_sync(0xFFFFFFFFu, ticket, 0);
+    if (ticket != ~0ull) {
+      if (lane == 0) {
+        const unsigned mask = (1u << ADDS_HUB_RING_LOG2) - 1u;
+        unsigned *seq = P.hub_seq + (ticket & mask);
+        Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
+        bool ok = true;
+        while (ld_acq32(seq) != (unsigned)(ticket + 1ull)) {
+          if (!w.spin(g, W_HUB_POP)) { ok = false; break; }
+        }
+        if (ok) {
+          const unsigned *hp = reinterpret_cast<const unsigned *>(P.hub + (ticket & mask));
+          HubChunk c;
+          c.q = __ldcg(hp);
+          c.du = __ldcg(hp + 1);
+          c.eb = __ldcg(hp + 2);
+          c.ee = __ldcg(hp + 3);
+          __threadfence();
+          st_rel32(seq, (unsigned)(ticket + (1ull << ADDS_HUB_RING_LOG2)));
+          S.status = ST_HUB;
+          S.q = c.q;
+          S.k = 1;
+          S.it_rb[0] = c.eb;
+          S.it_du[0] = c.du;
+          S.it_off[0] = 0;
+          S.total_edges = c.ee - c.eb;
+          const QueryCtl *ctl = P.qs[c.q].ctl;
+          const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
+          S.base_b = (unsigned)ctrl;
+          S.base_key = (unsigned)(ctrl >> 32);
+          S.shift = ld_rlx32(&ctl->shift);
+        } else {
+          S.status = ST_EXIT;
+        }
+      }
+      return;
+    }
+  }
+  /* 2. bucket queues, one query at a time starting at the sticky one */
+  unsigned q = S.cur_q;
+  const unsigned tries = P.nq < 8u ? P.nq : 8u;
+  for (unsigned t = 0; t < tries; ++t, q = (q + 1u == P.nq) ? 0u : q + 1u) {
+    const QueryDesc &d = P.qs[q];
+    QueryCtl *ctl = d.ctl;
+    if (ld_rlx32(&ctl->done) != 0u) continue;
+    const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
+    const unsigned base_b = (unsigned)ctrl;
+    const unsigned base_key = (unsigned)(ctrl >> 32);
+    const unsigned s = (base_b + lane) & (ADDS_NB - 1u);
+    SlotCtr *sc = d.slots + s;
+    const unsigned long long h = ld_rlx64(&sc->head);
+    const unsigned long long tl = ld_rlx64(&sc->tail);
+    const unsigned mask = __ballot_sync(0xFFFFFFFFu, tl > h);
+    if (mask == 0u) {
+      if (lane == 0 && ld_rlx32(&ctl->live) == 0u) {
+        if (atomicCAS(&ctl->done, 0u, 1u) == 0u) atomicSub(&g->remaining, 1u);
+      }
+      continue;
+    }
+    unsigned first = __ffs(mask) - 1u;
+    if (first > 0u) {
+      /* lowest bucket is empty: retire it (and the empty ones after it)
+       * unless strict ordering says its popped entries are still running */
+      const unsigned long long infl0 =
+          __shfl_sync(0xFFFFFFFFu, ld_rlx64(&sc->inflight), 0);
+      const bool drained = (P.strict_order == 0u) || (infl0 == 0ull);
+      if (drained) {
+        if (lane == 0) {
+          const unsigned long long nc =
+              ((unsigned long long)(base_key + first) << 32) | (base_b + first);
+          atomicCAS(&ctl->ctrl, ctrl, nc);
+        }
+      } else if (first >= P.window) {
+        continue; /* only work beyond the window: wait for the lowest bucket */
+      }
+    }
+    /* pop from slot base+first */
+    unsigned want = 0;
+    unsigned long long got = ~0ull;
+    if (lane == first) {
+      unsigned long long hh = h;
+      for (int r = 0; r < 4; ++r) {
+        const unsigned long long avail = tl - hh;
+        if (tl <= hh) break;
+        unsigned long long w = (avail + P.nctas - 1ull) / P.nctas;
+        if (w > P.batch_max) w = P.batch_max;
+        if (w == 0ull) w = 1ull;
+        const unsigned long long prev = atomicCAS(&sc->head, hh, hh + w);
+        if (prev == hh) { got = hh; want = (unsigned)w; break; }
+        hh = prev;
+      }
+      if (got != ~0ull) atomicAdd(&sc->inflight, (unsigned long long)want);
+    }
+    got = __shfl_sync(0xFFFFFFFFu, got, first);
+    want = __shfl_sync(0xFFFFFFFFu, want, first);
+    if (got == ~0ull) continue;
+    if (lane == 0) {
+      const unsigned long long vp0 = got >> ADDS_PAGE_LOG2;
+      const unsigned long long vp1 = (got + want - 1ull) >> ADDS_PAGE_LOG2;
+      const unsigned pi0 = pt_wait(P, d, (base_b + first) & (ADDS_NB - 1u), vp0, deadline);
+      const unsigned pi1 = (vp1 == vp0) ? pi0
+                           : pt_wait(P, d, (base_b + first) & (ADDS_NB - 1u), vp1, deadline);
+      S.status = ST_WORK;
+      S.q = q;
+      S.slot = (base_b + first) & (ADDS_NB - 1u);
+      S.h = got;
+      S.k = want;
+      S.pi0 = pi0;
+      S.pi1 = pi1;
+      const unsigned long long c2 = ld_rlx64(&ctl->ctrl);
+      S.base_b = (unsigned)c2;
+      S.base_key = (unsigned)(c2 >> 32);
+      S.shift = ld_rlx32(&ctl->shift);
+      S.cur_q = q;
+    }
+    return;
+  }
+  if (lane == 0) {
+    S.status = ST_IDLE;
+    S.cur_q = q;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Flush staged pushes: counting sort by bucket slot in shared memory, one
+ * tail reservation per non-empty slot, then the entry stores.  Replaces the
+ * per-warp match_any + atomicAdd + st.cg + __threadfence + write_done update
+ * of push_work (wl.h:1902-1928). */
+template <int BLOCK>
+__device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
+                      unsigned long long deadline, unsigned long long &st_pushes) {
+  const unsigned tid = threadIdx.x;
+  const unsigned cnt = S.pcnt;
+  if (cnt == 0u) return; /* uniform: read after a barrier */
+  if (tid < ADDS_NB) S.hist[tid] = 0u;
+  __syncthreads();
+  for (unsigned i = tid; i < cnt; i += BLOCK)
+    S.pb_rank[i] = (unsigned short)atomicAdd(&S.hist[S.pb_s[i]], 1u);
+  __syncthreads();
+  if (tid < 32u) {
+    const unsigned c = S.hist[tid];
+    if (tid == 0u) {
+      atomicAdd(&d.ctl->live, cnt); /* count before the entries are visible */
+      __threadfence();
+      st_pushes += cnt;
+    }
+    __syncwarp();
+    if (c != 0u) {
+      unsigned long long b;
+      unsigned p0, p1;
+      slot_reserve(P, d, tid, c, deadline, &b, &p0, &p1);
+      S.bbase[tid] = b;
+      S.bp0[tid] = p0;
+      S.bp1[tid] = p1;
+    }
+  }
+  __syncthreads();
+  for (unsigned i = tid; i < cnt; i += BLOCK) {
+    const unsigned s = S.pb_s[i];
+    const unsigned long long b = S.bbase[s];
+    const unsigned long long idx = b + S.pb_rank[i];
+    const unsigned pi = ((idx >> ADDS_PAGE_LOG2) == (b >> ADDS_PAGE_LOG2)) ? S.bp0[s] : S.bp1[s];
+    if (pi != PI_BAD) st_rlx64(entry_ptr(P, pi, idx), make_entry(S.pb_v[i], S.pb_d[i], pi));
+  }
+  __syncthreads();
+  if (tid == 0u) S.pcnt = 0u;
+  __syncthreads();
+}
+
+/* block-wide exclusive scan of one value per thread */
+template <int BLOCK>
+__device__ __forceinline__ unsigned block_exscan(Smem<BLOCK> &S, unsigned x, unsigned &total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  if (lane == 31u) S.wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = lane < BLOCK / 32 ? S.wsum[lane] : 0u;
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= (unsigned)o) wi += y;
+    }
+    if (lane < BLOCK / 32) S.wsum[lane] = wi - w;
+    if (lane == 31u) S.total_edges = wi;
+  }
+  __syncthreads();
+  total = S.total_edges;
+  return S.wsum[warp] + incl - x;
+}
+
+/* ------------------------------------------------------------------------ */
+/* the persistent solver                                                      */
+template <bool FLT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<BLOCK> &S = *reinterpret_cast<Smem<BLOCK> *>(smem_raw);
+  constexpr int U = Smem<BLOCK>::U;
+  constexpr unsigned FLUSH_AT = Smem<BLOCK>::SB - BLOCK * U;
+  const unsigned tid = threadIdx.x;
+  const unsigned long long deadline = gtimer() + P.timeout_ns;
+
+  unsigned long long st_items = 0, st_stale = 0, st_edges = 0, st_pushes = 0,
+                     st_batches = 0, st_hub = 0;
+  if (tid == 0) {
+    S.cur_q = blockIdx.x % P.nq;
+    S.pcnt = 0;
+    S.idle = 0;
+    S.hub_chunks = 0;
+  }
+  __syncthreads();
+
+  for (;;) {
+    if (tid < 32) acquire<BLOCK>(P, S, deadline);
+    __syncthreads();
+    const unsigned status = S.status;
+    if (status == ST_EXIT) break;
+    if (status == ST_IDLE) {
+      if (tid == 0) {
+        const unsigned n = ++S.idle;
+        if (gtimer() > deadline) raise_err(P.g, ADDS_DEV_TIMEOUT, W_IDLE);
+        __nanosleep(n < 8 ? 100 : (n < 64 ? 400 : 1000));
+      }
+      __syncthreads();
+      continue;
+    }
+    if (tid == 0) S.idle = 0;
+    const unsigned q = S.q;
+    const QueryDesc &d = P.qs[q];
+    const unsigned *__restrict__ row = d.row;
+    const uint2 *__restrict__ edges = d.edges;
+    unsigned *dist = d.dist;
+    const float scale = d.scale;
+    const unsigned shift = S.shift, base_b = S.base_b, base_key = S.base_key;
+    unsigned k = 1;
+
+    if (status == ST_WORK) {
+      k = S.k;
+      const unsigned long long h = S.h;
+      unsigned deg = 0, rb = 0, dp = 0, chunks = 0;
+      if (tid < k) {
+        const unsigned long long idx = h + tid;
+        const unsigned pi = ((idx >> ADDS_PAGE_LOG2) == (h >> ADDS_PAGE_LOG2)) ? S.pi0 : S.pi1;
+        bool ok = pi != PI_BAD;
+        unsigned long long e = 0;
+        if (ok) {
+          const unsigned long long *ep = entry_ptr(P, pi, idx);
+          Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
+          e = ld_rlx64(ep);
+          while (((unsigned)e & 0x80000000u) != (pi & 0x80000000u)) {
+            if (!w.spin(P.g, W_ENTRY)) { ok = false; break; }
+            e = ld_rlx64(ep);
+          }
+        }
+        if (ok) {
+          const unsigned v = (unsigned)e & 0x7FFFFFFFu;
+          dp = (unsigned)(e >> 32);
+          const unsigned dv = __ldcg(dist + v);
+          ++st_items;
+          if (dv < dp) {
+            ++st_stale; /* superseded: a later push carries the smaller value */
+          } else {
+            rb = __ldg(row + v);
+            const unsigned re = __ldg(row + v + 1);
+            deg = re - rb;
+            if (deg > P.hub_threshold) {
+              chunks = (deg + P.hub_chunk - 1u) / P.hub_chunk;
+              atomicAdd(&S.hub_chunks, chunks);
+            } else {
+              st_edges += deg; /* split rows are counted chunk by chunk */
+            }
+          }
+        }
+      }
+      S.it_rb[tid] = rb;
+      S.it_du[tid] = dp;
+      unsigned tot;
+      const unsigned off = block_exscan<BLOCK>(S, chunks ? 0u : deg, tot);
+      S.it_off[tid] = off;
+      /* retire the popped range: pages whose entries are all consumed go back */
+      if (tid == 0) {
+        const unsigned c0 = min((unsigned)(ADDS_PAGE - (h & PAGE_MASK)), k);
+        consume(P, S.pi0, c0);
+        if (k > c0) consume(P, S.pi1, k - c0);
+        if (S.hub_chunks) {
+          atomicAdd(&d.ctl->live, S.hub_chunks);
+          __threadfence();
+        }
+      }
+      __syncthreads();
+      if (chunks) {
+        /* publish this row's chunks for the whole grid (tb_coop_assign,
+         * wl.h:1638-1696, widened from one block to all CTAs) */
+        const unsigned mask = (1u << ADDS_HUB_RING_LOG2) - 1u;
+        const unsigned long long t0 = atomicAdd(&P.g->hub_tail, (unsigned long long)chunks);
+        for (unsigned c = 0; c < chunks; ++c) {
+          const unsigned long long t = t0 + c;
+          unsigned *seq = P.hub_seq + (t & mask);
+          Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
+          bool ok = true;
+          while (ld_acq32(seq) != (unsigned)t) {
+            if (!w.spin(P.g, W_HUB_PUB)) { ok = false; break; }
+          }
+          if (!ok) break;
+          HubChunk hc;
+          hc.q = q;
+          hc.du = dp;
+          hc.eb = rb + c * P.hub_chunk;
+          hc.ee = (unsigned)min((unsigned long long)rb + (unsigned long long)(c + 1u) * P.hub_chunk,
+                                (unsigned long long)rb + deg);
+          P.hub[t & mask] = hc;
+          __threadfence();
+          st_rel32(seq, (unsigned)(t + 1ull));
+        }
+      }
+    } else { /* ST_HUB: one chunk of a split row, staged by acquire */
+      if (tid == 0) {
+        ++st_hub;
+        st_edges += S.total_edges;
+      }
+    }
+    if (tid == 0) {
+      ++st_batches;
+      S.hub_chunks = 0;
+    }
+
+    /* edge-balanced expansion of the batch: relax + atomicMin + stage push */
+    const unsigned E = S.total_edges;
+    for (unsigned eb = 0; eb < E; eb += BLOCK * U) {
+      unsigned dst[U], nd[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const unsigned e = eb + u * BLOCK + tid;
+        nd[u] = 0xFFFFFFFFu;
+        dst[u] = 0;
+        if (e < E) {
+          int lo = 0, hi = (int)k - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (S.it_off[mid] <= e) lo = mid; else hi = mid - 1;
+          }
+          const uint2 ed = __ldg(edges + S.it_rb[lo] + (e - S.it_off[lo]));
+          const unsigned du = S.it_du[lo];
+          dst[u] = ed.x;
+          nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(ed.y)))
+                      : du + ed.y;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (nd[u] != 0xFFFFFFFFu) {
+          const unsigned cur = __ldcg(dist + dst[u]);
+          if (nd[u] < cur) {
+            const unsigned old = atomicMin(dist + dst[u], nd[u]);
+            if (old > nd[u]) {
+              const unsigned s =
+                  bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key);
+              cg::coalesced_group grp = cg::coalesced_threads();
+              unsigned pos = 0;
+              if (grp.thread_rank() == 0) pos = atomicAdd(&S.pcnt, grp.size());
+              pos = grp.shfl(pos, 0) + grp.thread_rank();
+              S.pb_v[pos] = dst[u];
+              S.pb_d[pos] = nd[u];
+              S.pb_s[pos] = (unsigned char)s;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, S, d, deadline, st_pushes);
+    }
+    __syncthreads();
+    flush<BLOCK>(P, S, d, deadline, st_pushes);
+    /* batch finished: its k entries (or one chunk) leave the live count */
+    if (tid == 0) {
+      if (status == ST_WORK) atomicAdd(&d.slots[S.slot].inflight, (unsigned long long)(0ull - k));
+      atomicSub(&d.ctl->live, k);
+    }
+    __syncthreads();
+  }
+
+  /* statistics */
+  {
+    GlobalCtl *g = P.g;
+#define WSUM(x) \
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+    WSUM(st_items) WSUM(st_stale) WSUM(st_edges) WSUM(st_pushes)
+#undef WSUM
+    if ((tid & 31u) == 0u) {
+      if (st_items) atomicAdd(&g->st_items, st_items);
+      if (st_stale) atomicAdd(&g->st_stale, st_stale);
+      if (st_edges) atomicAdd(&g->st_edges, st_edges);
+      if (st_pushes) atomicAdd(&g->st_pushes, st_pushes);
+      if (tid == 0) {
+        if (st_hub) atomicAdd(&g->st_hub, st_hub);
+        atomicAdd(&g->st_batches, st_batches);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* init: d = INF, d[src] = 0, per-query control reset, source pushed to the
+ * lowest bucket (ads_int/kernel.cu:18-27 + assign_manager's source push,
+ * wl.h:944-953).  grid = (x, nq). */
+__global__ void init_kernel(EngParams P) {
+  const unsigned q = blockIdx.y;
+  const QueryDesc &d = P.qs[q];
+  const unsigned src = (P.single_src != 0xFFFFFFFFu && q == 0u) ? P.single_src : d.src;
+  const unsigned inf = P.is_float ? ADDS_INF_F32_BITSV : ADDS_INF_I32_BITS;
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < d.n;
+       v += gridDim.x * blockDim.x)
+    d.dist[v] = (v == src) ? 0u : inf;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    GlobalCtl *g = P.g;
+    if (q == 0) {
+      g->remaining = P.nq;
+      g->st_items = g->st_stale = g->st_edges = g->st_pushes = 0;
+      g->st_batches = g->st_hub = 0;
+    }
+    QueryCtl *c = d.ctl;
+    c->ctrl = 0ull;
+    c->done = 0u;
+    c->shift = d.shift0;
+    c->adapt_state = 0u;
+    c->pushes_at_base = 0ull;
+    for (int s = 0; s < ADDS_NB; ++s) d.slots[s].inflight = 0ull;
+    c->live = 1u;
+    __threadfence();
+    const unsigned long long deadline = gtimer() + P.timeout_ns;
+    unsigned long long b;
+    unsigned p0, p1;
+    if (slot_reserve(P, d, 0u, 1u, deadline, &b, &p0, &p1))
+      st_rlx64(entry_ptr(P, p0, b), make_entry(src, 0u, p0));
+  }
+}
+
+/* reached vertices and their out-edges (m_r, n_r of the GTEPS metric) */
+__global__ void reached_kernel(const unsigned *row, const unsigned *dist, unsigned n,
+                               unsigned inf, unsigned long long *out) {
+  unsigned long long nr = 0, mr = 0;
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    if (dist[v] != inf) {
+      ++nr;
+      mr += row[v + 1] - row[v];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    nr += __shfl_down_sync(0xFFFFFFFFu, nr, o);
+    mr += __shfl_down_sync(0xFFFFFFFFu, mr, o);
+  }
+  if ((threadIdx.x & 31u) == 0u) {
+    atomicAdd(out, nr);
+    atomicAdd(out + 1, mr);
+  }
+}
+
+/* worklist full reset: free queue holds every page, hub ring sequence = i */
+__global__ void wl_reset_kernel(unsigned long long *fq, unsigned fq_cells, unsigned pool_pages,
+                                unsigned *hub_seq, unsigned hub_cells) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < fq_cells;
+       i += gridDim.x * blockDim.x)
+    fq[i] = (i < pool_pages) ? (((unsigned long long)i << 32) | i)
+                             : (unsigned long long)(~i); /* tag never equals i */
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < hub_cells;
+       i += gridDim.x * blockDim.x)
+    hub_seq[i] = i;
+}
+
+/* ------------------------------------------------------------------------ */
+/* host-side launch helpers (called from api.cu)                              */
+static const int kBlock = 512;
+
+template <bool FLT>
+static cudaError_t prep_solver(int *max_blocks_per_sm) {
+  const size_t smem = sizeof(Smem<kBlock>);
+  cudaError_t e = cudaFuncSetAttribute(solve_kernel<FLT, kBlock>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
+                                                       solve_kernel<FLT, kBlock>, kBlock, smem);
+}
+
+}  // namespace adds
+
+/* C++ linkage entry points used by api.cu */
+cudaError_t adds_engine_prepare(bool flt, int *max_blocks_per_sm, int *block) {
+  *block = adds::kBlock;
+  return flt ? adds::prep_solver<true>(max_blocks_per_sm)
+             : adds::prep_solver<false>(max_blocks_per_sm);
+}
+
+cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStream_t st) {
+  unsigned bx = (max_n + 1023u) / 1024u;
+  if (bx > 1184u) bx = 1184u; /* 8 x 148 SMs: grid-stride beyond that */
+  if (bx == 0u) bx = 1u;
+  dim3 grid(bx, P.nq);
+  adds::init_kernel<<<grid, 1024, 0, st>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t adds_engine_launch_solve(const EngParams &P, cudaStream_t st) {
+  /* cooperative launch: all CTAs co-resident (they wait on each other's
+   * pushes); cudaLaunchKernelEx form so the launch can be graph-captured */
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.nctas);
+  cfg.blockDim = dim3(adds::kBlock);
+  cfg.dynamicSmemBytes = sizeof(adds::Smem<adds::kBlock>);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (P.is_float) return cudaLaunchKernelEx(&cfg, adds::solve_kernel<true, adds::kBlock>, P);
+  return cudaLaunchKernelEx(&cfg, adds::solve_kernel<false, adds::kBlock>, P);
+}
+
+cudaError_t adds_engine_launch_reached(const unsigned *row, const unsigned *dist, unsigned n,
+                                       unsigned inf, unsigned long long *out, cudaStream_t st) {
+  unsigned bx = (n + 255u) / 256u;
+  if (bx > 1184u) bx = 1184u;
+  if (bx == 0u) bx = 1u;
+  adds::reached_kernel<<<bx, 256, 0, st>>>(row, dist, n, inf, out);
+  return cudaGetLastError();
+}
+
+cudaError_t adds_engine_launch_reset(unsigned long long *fq, unsigned fq_cells,
+                                     unsigned pool_pages, unsigned *hub_seq, unsigned hub_cells,
+                                     cudaStream_t st) {
+  adds::wl_reset_kernel<<<296, 256, 0, st>>>(fq, fq_cells, pool_pages, hub_seq, hub_cells);
+  return cudaGetLastError();
+}

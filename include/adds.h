@@ -1,0 +1,221 @@
+/*
+ * adds.h — C ABI of the B200-native asynchronous delta-stepping SSSP engine.
+ *
+ * The reference (UCLA-VAST/adds) has no library API: its only boundary is the
+ * `sssp` process (ads_int/support.cu:11-76, ads_int/kernel.cu:290-305) plus the
+ * CSR graph object handed to gg_main (ads_int/kernel.cu:185) and the host half
+ * of the worklist (ads_int/wl.h:160-165).  Every entry point below names the
+ * reference interface it replaces.  All functions return 0 (ADDS_OK) or a
+ * negative ADDS_ERR_* code; none of them calls exit() or traps on the device.
+ *
+ * Conventions
+ *   - Vertex ids are uint32 (reference index_type is `unsigned`,
+ *     ads_int/csr_graph.h:20); edge counts must be < 2^32 for the same reason.
+ *   - Distances are 32-bit words: int32 for ADDS_I32 graphs (INF = INT32_MAX,
+ *     ads_int/csr_graph.h:23) and float32 for ADDS_F32 graphs
+ *     (INF = FLT_MAX, ads_float/csr_graph.h:49).
+ *   - Weights must be non-negative (int32 in [0, INT32_MAX], float32 >= 0 and
+ *     not NaN).  -0.0f is stored as +0.0f (same sums).
+ *   - A pointer argument documented as "host or device" is classified with
+ *     cudaPointerGetAttributes; device pointers must live on the graph's GPU.
+ *   - Handles are not thread-safe: concurrent calls on one handle race;
+ *     distinct handles may be used from distinct threads.
+ */
+#ifndef ADDS_H_
+#define ADDS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADDS_ABI_VERSION 1
+
+typedef enum { ADDS_I32 = 0, ADDS_F32 = 1 } adds_wtype;
+
+enum {
+  ADDS_OK = 0,
+  ADDS_ERR_INVALID = -1,        /* bad argument                                  */
+  ADDS_ERR_IO = -2,             /* file could not be opened/read/written         */
+  ADDS_ERR_FORMAT = -3,         /* malformed .gr file                             */
+  ADDS_ERR_OOM = -4,            /* device or host allocation failed               */
+  ADDS_ERR_CUDA = -5,           /* a CUDA runtime call failed                     */
+  ADDS_ERR_DEVICE_TIMEOUT = -6, /* a bounded device wait ran out                  */
+  ADDS_ERR_WL_OVERFLOW = -7,    /* worklist pool exhausted after all regrowths    */
+  ADDS_ERR_NO_DEVICE = -8,      /* no usable sm_100 device                        */
+  ADDS_ERR_UNSUPPORTED = -9     /* request outside what this build supports       */
+};
+
+#define ADDS_INF_I32 0x7FFFFFFF
+#define ADDS_INF_F32_BITS 0x7F7FFFFFu /* FLT_MAX */
+
+typedef struct adds_graph adds_graph; /* device-resident CSR, library-owned */
+typedef struct adds_batch adds_batch; /* many solves in one persistent launch */
+
+/* Solver knobs.  Zero / negative means "choose automatically".
+ * Replaces the compile-time tuning of ads_int/wl.h:14-25,777-849 and the
+ * runtime delta choice of worklist::set_param (ads_int/wl.h:395-449). */
+typedef struct adds_opts {
+  void *stream;          /* cudaStream_t to run on; NULL = per-graph stream      */
+  int32_t delta_shift;   /* bucket width 2^shift key units; <0 = auto            */
+  float delta_scale;     /* float graphs: key = floor(dist*scale); <=0 = auto   */
+  int32_t window;        /* buckets popped concurrently (1..32); 0 = auto        */
+  int32_t ctas_per_sm;   /* persistent CTAs per SM; 0 = auto                     */
+  int32_t batch_max;     /* max vertices one CTA pops per batch; 0 = auto        */
+  int32_t hub_threshold; /* out-degree above which a row is split across CTAs   */
+  int32_t timeout_ms;    /* bound on every device wait; 0 = 20000 ms             */
+  int32_t adapt;         /* on-device delta re-tuning: -1 auto, 0 off, 1 on      */
+  int32_t strict_order;  /* 1: advance a bucket only when its work is done       */
+  int32_t reserved[6];
+} adds_opts;
+
+/* Per-solve statistics (reference: work_count + fd-3 record,
+ * ads_int/kernel.cu:264-282). */
+typedef struct adds_stats {
+  double ms;                /* device time of the solve(s), CUDA events        */
+  uint64_t items_popped;    /* queue entries popped (reference int work count) */
+  uint64_t items_stale;     /* popped entries skipped as superseded            */
+  uint64_t edges_scanned;   /* edges of expanded vertices (float work count)   */
+  uint64_t pushes;          /* queue entries pushed                            */
+  uint64_t batches;         /* CTA-level pops                                  */
+  uint64_t hub_chunks;      /* split row chunks processed                      */
+  uint64_t reached;         /* vertices with finite distance (filled on request) */
+  uint64_t reached_edges;   /* out-edges of reached vertices (filled on request) */
+  int32_t delta_shift;      /* bucket shift at the end of the solve            */
+  int32_t retries;          /* worklist regrowths needed                       */
+  int32_t ctas;             /* persistent CTAs launched                        */
+  int32_t reserved[5];
+} adds_stats;
+
+typedef struct adds_graph_info_t {
+  uint32_t n;
+  uint64_t m;
+  adds_wtype wtype;
+  int device;
+  uint32_t max_degree;
+  double avg_degree;
+  double avg_weight;      /* sampled mean weight (as ads_int/kernel.cu:153-183) */
+  uint64_t device_bytes;  /* bytes held on the GPU by the graph                  */
+} adds_graph_info_t;
+
+/* ---- library ------------------------------------------------------------ */
+int adds_abi_version(void);
+const char *adds_strerror(int code);
+void adds_opts_init(adds_opts *o);
+/* Last CUDA error text seen by this thread (diagnostics only). */
+const char *adds_last_cuda_error(void);
+
+/* ---- graphs ------------------------------------------------------------- */
+/* Replaces CSRGraph::read/readFromGR + copy_to_gpu
+ * (ads_int/csr_graph.cu:203-296,309-328; float: ads_float/csr_graph.cu).
+ * Galois .gr v1 layout: u64 version=1, u64 sizeEdgeTy, u64 n, u64 m,
+ * u64 out_end[n], u32 dst[m], (u32 pad if m odd), u32|f32 w[m].
+ * sizeEdgeTy==0 gives all-zero weights, as the reference does. */
+int adds_graph_load_gr(const char *path, adds_wtype wt, int device,
+                       adds_graph **out);
+/* Builds a device graph from host CSR arrays (copied; caller keeps them).
+ * row_start has n+1 entries, row_start[0]==0, row_start[n]==m. */
+int adds_graph_from_csr(uint32_t n, uint64_t m, const uint64_t *row_start,
+                        const uint32_t *dst, const void *w, adds_wtype wt,
+                        int device, adds_graph **out);
+int adds_graph_info(const adds_graph *g, adds_graph_info_t *info);
+/* Copies the CSR back to host buffers (any may be NULL).  Replaces
+ * CSRGraph::copy_to_cpu (ads_int/csr_graph.cu:330-350) minus the distances. */
+int adds_graph_download(const adds_graph *g, uint64_t *row_start, uint32_t *dst,
+                        void *w);
+/* Overwrites the m edge weights (host or device pointer, CSR order). */
+int adds_graph_set_weights(adds_graph *g, const void *w);
+/* Writes the graph as a Galois .gr v1 file (input side of run_all.sh). */
+int adds_graph_save_gr(const adds_graph *g, const char *path);
+void adds_graph_free(adds_graph *g);
+
+/* Seeded synthetic generators, run on the GPU; identical to the numpy
+ * generators in adds_b200/graphs.py.  kind: 0 = R-MAT, 1 = 2-D grid with
+ * local shortcuts, 2 = Erdos-Renyi, 3 = plain 2-D grid. */
+typedef struct adds_gen_spec {
+  int32_t kind;
+  int32_t scale;        /* R-MAT: n = 2^scale                                 */
+  int32_t edge_factor;  /* R-MAT / ER: directed draws = edge_factor * n       */
+  uint32_t n;           /* ER: vertex count                                   */
+  uint32_t side_x, side_y; /* grids                                           */
+  double a, b, c;       /* R-MAT quadrant probabilities (d = 1-a-b-c)         */
+  double shortcut_frac; /* grid: shortcut pairs = frac * grid edges           */
+  int32_t shortcut_radius;
+  adds_wtype wtype;
+  double w_lo, w_hi;    /* int: uniform [lo,hi]; float: uniform [lo,hi)       */
+  uint64_t seed;
+} adds_gen_spec;
+int adds_graph_generate(const adds_gen_spec *spec, int device, adds_graph **out);
+
+/* ---- plain solve -------------------------------------------------------- */
+/* One SSSP from src.  Replaces gg_main's solve (ads_int/kernel.cu:185-288):
+ * init kernel, profiler_kernel + set_param delta choice, and the
+ * driver_kernel/wl_kernel/sssp_kernel pair, as one init + one persistent
+ * cooperative launch.  dist_out (n words, host or device) may be NULL to keep
+ * the result on the device (read it with adds_graph_last_dist). */
+int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds_opts *opts,
+              adds_stats *stats);
+/* Enqueues a solve on the graph's stream and returns at once (no host
+ * synchronisation); adds_graph_sync waits for all enqueued solves and
+ * reports the first device error.  The distances of the last solve stay in
+ * the graph. */
+int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opts);
+int adds_graph_sync(adds_graph *g, adds_stats *stats);
+/* Copies the distances of the last solve on g (host or device pointer). */
+int adds_graph_last_dist(adds_graph *g, void *dist_out);
+/* Fills stats->reached and stats->reached_edges for the last solve on g. */
+int adds_graph_reached(adds_graph *g, uint64_t *reached, uint64_t *reached_edges);
+
+/* ---- batched solves ----------------------------------------------------- */
+/* nq solves (graph graphs[i], source srcs[i]) run in ONE persistent launch
+ * with per-query bucket queues sharing one page pool; the launch is captured
+ * in a CUDA graph on first run and replayed afterwards.  No reference
+ * counterpart (the reference runs one source per process). */
+int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs,
+                      uint32_t nq, const adds_opts *opts, adds_batch **out);
+int adds_batch_run(adds_batch *b, adds_stats *stats);
+/* Enqueues a run on the batch's stream without waiting; adds_batch_sync
+ * waits and reports device errors. */
+int adds_batch_launch(adds_batch *b);
+int adds_batch_sync(adds_batch *b, adds_stats *stats);
+int adds_batch_dist(adds_batch *b, uint32_t q, void *dist_out);
+/* Device pointer to query q's distance array (valid until adds_batch_free). */
+int adds_batch_dist_ptr(adds_batch *b, uint32_t q, void **dptr);
+int adds_batch_set_sources(adds_batch *b, const uint32_t *srcs);
+void adds_batch_free(adds_batch *b);
+
+/* ---- adjoint (backward) ------------------------------------------------- */
+/* Float graphs only.  For every query q of the batch, takes dL/d dist_q
+ * (n_q floats, device pointer) and ACCUMULATES dL/dw into grad_w[g] (m_g
+ * floats, device pointer) for each distinct graph, summing over queries in
+ * query order.  The predecessor of v is the tight in-edge (u->v) with
+ * fl(d[u]+w)==d[v] and d[u]<d[v] of smallest CSR index; zero-gap ties are
+ * resolved breadth-first, again by smallest index.  No reference counterpart. */
+int adds_batch_backward(adds_batch *b, const float *const *grad_dist,
+                        float *const *grad_w);
+/* Single-graph convenience: ns solves from srcs, dist/grad_dist are [ns][n]
+ * device arrays laid out row-major, grad_w (m floats, device) is overwritten. */
+int adds_sssp_backward(adds_graph *g, uint32_t ns, const uint32_t *srcs,
+                       const float *dist, const float *grad_dist, float *grad_w,
+                       const adds_opts *opts);
+
+/* ---- autotuner ---------------------------------------------------------- */
+/* Times candidate (delta, window, CTAs/SM, batch, hub threshold) settings on
+ * the sample sources and stores the fastest in the graph (used whenever a
+ * later call passes "auto" knobs).  best may be NULL. */
+int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns,
+              adds_opts *best, double *best_ms);
+
+/* ---- text output -------------------------------------------------------- */
+/* Writes n lines "<v> <dist>" / "<v> INF" exactly as support.cu:78-97 (int,
+ * "%d %d") and the Galois float writer (cpu_sssp_float.patch:241-247,
+ * "%d %f").  dist is a host array of 32-bit words. */
+int adds_write_dist_text(const char *path, uint32_t n, const void *dist,
+                         adds_wtype wt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADDS_H_ */
