@@ -51,19 +51,28 @@ class Opts(C.Structure):
         ("timeout_ms", C.c_int32),
         ("adapt", C.c_int32),
         ("strict_order", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("local_max", C.c_int32),
+        ("light_heavy", C.c_int32),
+        ("block_threads", C.c_int32),
+        ("greed", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 
 class Stats(C.Structure):
     _fields_ = [
         ("ms", C.c_double),
+        ("kernel_ms", C.c_double),
         ("items_popped", C.c_uint64),
         ("items_stale", C.c_uint64),
         ("edges_scanned", C.c_uint64),
         ("pushes", C.c_uint64),
         ("batches", C.c_uint64),
         ("hub_chunks", C.c_uint64),
+        ("hub_stale", C.c_uint64),
+        ("local_batches", C.c_uint64),
+        ("heavy_lists", C.c_uint64),
+        ("phase_cycles", C.c_uint64 * 6),
         ("reached", C.c_uint64),
         ("reached_edges", C.c_uint64),
         ("delta_shift", C.c_int32),
@@ -73,7 +82,9 @@ class Stats(C.Structure):
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "phase_cycles")}
+        d["phase_cycles"] = list(self.phase_cycles)
+        return d
 
 
 class GraphInfo(C.Structure):

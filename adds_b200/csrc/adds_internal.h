@@ -30,18 +30,30 @@
 #define ADDS_DEV_HUB_OVERFLOW 3u
 
 /* One bucket slot: monotone 64-bit virtual indices.  Entries [head, tail)
- * are pushed but not popped.  inflight counts popped-but-unfinished entries
- * (used only to decide when the lowest bucket may be retired). */
-struct __align__(32) SlotCtr {
+ * are reserved by pushers; `avail` counts reserved, written entries that no
+ * popper has claimed yet (pushers add after their stores, poppers claim by
+ * fetch-and-subtract, so no popper ever takes an index that was not
+ * reserved).  inflight counts claimed-but-unfinished entries (used only to
+ * decide when the lowest bucket may be retired).  Each counter has its own
+ * 32-byte sector so the fetch-and-adds on them do not share a sector. */
+struct __align__(128) SlotCtr {
   unsigned long long head;
+  unsigned long long pad0[3];
   unsigned long long tail;
+  unsigned long long pad1[3];
+  long long avail;
+  unsigned long long pad2[3];
   unsigned long long inflight;
-  unsigned long long pad;
+  unsigned long long pad3[3];
 };
 
-/* Per-query mutable control, one 128-byte line each. */
+/* Per-query mutable control, one 128-byte line each.  ctrl packs the lowest
+ * live bucket: low word = base bucket counter (31 bits) | phase << 31 (0:
+ * its light edges are being relaxed, 1: its settled vertices' heavy edges
+ * are), high word = the base bucket's key (dist key >> shift). */
+#define ADDS_PHASE_H 0x80000000u
 struct __align__(128) QueryCtl {
-  unsigned long long ctrl; /* (base_key << 32) | base_bucket                  */
+  unsigned long long ctrl;
   unsigned live;           /* entries pushed (queue or hub ring) not finished   */
   unsigned done;           /* 1 once live reached 0                            */
   unsigned shift;          /* current bucket shift (device-adapted)            */
@@ -53,24 +65,28 @@ struct __align__(128) QueryCtl {
 /* Read-only per-query descriptor. */
 struct QueryDesc {
   const unsigned *row;     /* n+1 row offsets (u32)                           */
-  const uint2 *edges;      /* m x {dst, weight bits}                          */
+  const uint2 *edges;      /* m x {dst, weight bits}, rows sorted by weight   */
+  const unsigned *split;   /* per vertex: count of light edges (w < delta) at
+                              the start of its row; NULL = every edge light  */
   unsigned *dist;          /* n distance words                                */
   unsigned n;
   unsigned src;
   float scale;             /* float graphs: key = floor(d*scale)              */
   unsigned ptn_log2;       /* page-table ring size per slot (log2)            */
-  unsigned long long *pt;  /* [ADDS_NB << ptn_log2] page-table entries        */
-  SlotCtr *slots;          /* [ADDS_NB]                                       */
+  unsigned long long *pt;  /* [2*ADDS_NB << ptn_log2] page-table entries      */
+  SlotCtr *slots;          /* [2*ADDS_NB]: light buckets, then heavy lists    */
   QueryCtl *ctl;
   unsigned shift0;         /* initial bucket shift                            */
   unsigned graph_id;       /* index of the distinct graph (backward pass)     */
 };
 
-struct HubChunk {          /* a slice of one long row                         */
+struct __align__(32) HubChunk { /* a slice of one long row                    */
   unsigned q;
+  unsigned u;                   /* the row's vertex: stale chunks are skipped */
   unsigned du;
   unsigned eb;
   unsigned ee;
+  unsigned pad[3];
 };
 
 /* Engine-wide control block. */
@@ -83,6 +99,8 @@ struct __align__(128) GlobalCtl {
   unsigned long long fq_tail; unsigned long long pad2[15];
   unsigned long long hub_head; unsigned long long pad3[15]; /* chunk ring     */
   unsigned long long hub_tail; unsigned long long pad4[15];
+  unsigned hungry;          /* CTAs currently without work                   */
+  unsigned pad5[31];
   /* statistics */
   unsigned long long st_items;
   unsigned long long st_stale;
@@ -90,7 +108,12 @@ struct __align__(128) GlobalCtl {
   unsigned long long st_pushes;
   unsigned long long st_batches;
   unsigned long long st_hub;
-  unsigned long long st_pad[10];
+  unsigned long long st_local;   /* batches taken from the CTA's own pushes     */
+  unsigned long long st_hub_stale;
+  unsigned long long st_heavy;    /* heavy-edge lists expanded                   */
+  unsigned long long st_cyc[6];   /* SM cycles: acquire, load, edges, flush,
+                                     idle, total (summed over CTAs)            */
+  unsigned long long st_pad[1];
 };
 
 /* Kernel parameters (passed by value). */
@@ -117,6 +140,10 @@ struct EngParams {
   unsigned adapt;
   unsigned is_float;
   unsigned single_src;          /* init: override source of query 0 if != ~0 */
+  unsigned local_max;           /* own pushes kept as the next batch         */
+  unsigned local_max_hungry;    /* ... while other CTAs are waiting for work */
+  unsigned block;               /* threads per CTA (selects the kernel)      */
+  unsigned greed;               /* claim share = avail / (nctas >> greed)    */
 };
 
 #endif /* ADDS_INTERNAL_H_ */

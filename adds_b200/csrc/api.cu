@@ -9,6 +9,7 @@
  * regrows and the solve reruns when the device reports overflow, and the
  * launch is one cooperative persistent kernel instead of CDP children.
  */
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <fcntl.h>
@@ -27,9 +28,9 @@
 #include "adds_internal.h"
 
 /* engine.cu */
-cudaError_t adds_engine_prepare(bool flt, int *max_blocks_per_sm, int *block);
+cudaError_t adds_engine_prepare(bool flt, int block, int *max_blocks_per_sm);
 cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStream_t st);
-cudaError_t adds_engine_launch_solve(const EngParams &P, cudaStream_t st);
+cudaError_t adds_engine_launch_solve(const EngParams &P, int block, cudaStream_t st);
 cudaError_t adds_engine_launch_reached(const unsigned *row, const unsigned *dist, unsigned n,
                                        unsigned inf, unsigned long long *out, cudaStream_t st);
 cudaError_t adds_engine_launch_reset(unsigned long long *fq, unsigned fq_cells,
@@ -85,6 +86,10 @@ extern "C" void adds_opts_init(adds_opts *o) {
   o->delta_scale = 0.f;
   o->adapt = -1;
   o->strict_order = -1;
+  o->local_max = -1;
+  o->light_heavy = -1;
+  o->block_threads = 0;
+  o->greed = -1;
 }
 
 static unsigned next_pow2(unsigned long long x) {
@@ -98,6 +103,7 @@ static unsigned next_pow2(unsigned long long x) {
 struct EngQuery {
   const unsigned *row;
   const uint2 *edges;
+  const unsigned *split;
   unsigned *dist;
   unsigned n;
   unsigned long long m;
@@ -126,8 +132,11 @@ struct Engine {
   GlobalCtl *g_host = nullptr; /* pinned */
   std::vector<QueryDesc> qs_host;
   size_t bytes = 0;
-  int block = 0, max_bps = 0, num_sms = 0;
+  int max_bps[3] = {0, 0, 0}; /* resident CTAs per SM for 128/256/512 threads */
+  int num_sms = 0;
 };
+
+static int block_index(int block) { return block == 128 ? 0 : (block == 256 ? 1 : 2); }
 
 static void engine_free(Engine &E) {
   void *ptrs[] = {E.pool, E.pgen, E.pcons, E.fq, E.hub, E.hub_seq, E.g, E.qs, E.ctl, E.slots, E.pt, E.reach};
@@ -143,10 +152,10 @@ static int engine_full_reset(Engine &E, cudaStream_t st) {
   CK(cudaMemsetAsync(E.pgen, 0, (size_t)E.pool_pages * 4, st));
   CK(cudaMemsetAsync(E.pcons, 0, (size_t)E.pool_pages * 4, st));
   CK(cudaMemsetAsync(E.g, 0, sizeof(GlobalCtl), st));
-  CK(cudaMemsetAsync(E.slots, 0, (size_t)E.nq * ADDS_NB * sizeof(SlotCtr), st));
+  CK(cudaMemsetAsync(E.slots, 0, (size_t)E.nq * 2 * ADDS_NB * sizeof(SlotCtr), st));
   CK(cudaMemsetAsync(E.ctl, 0, (size_t)E.nq * sizeof(QueryCtl), st));
   size_t pt_words = 0;
-  for (auto &q : E.qs_host) pt_words += (size_t)ADDS_NB << q.ptn_log2;
+  for (auto &q : E.qs_host) pt_words += (size_t)2 * ADDS_NB << q.ptn_log2;
   CK(cudaMemsetAsync(E.pt, 0xFF, pt_words * 8, st));
   const unsigned long long tail = E.pool_pages;
   CK(cudaMemcpyAsync(&E.g->fq_tail, &tail, 8, cudaMemcpyHostToDevice, st));
@@ -169,15 +178,18 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
   E.device = device;
   E.flt = flt;
   E.nq = (unsigned)qv.size();
-  CK(adds_engine_prepare(flt, &E.max_bps, &E.block));
+  for (int i = 0; i < 3; ++i) {
+    CK(adds_engine_prepare(flt, 128 << i, &E.max_bps[i]));
+    if (E.max_bps[i] < 1) return ADDS_ERR_UNSUPPORTED; /* variant cannot be resident */
+  }
   CK(cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device));
-  if (E.max_bps < 1 || E.num_sms < 1) return ADDS_ERR_UNSUPPORTED; /* kernel cannot be resident */
+  if (E.num_sms < 1) return ADDS_ERR_UNSUPPORTED;
   double sum_need = 0;
   E.qs_host.resize(E.nq);
   size_t pt_words = 0;
   for (unsigned i = 0; i < E.nq; ++i) {
     const EngQuery &q = qv[i];
-    const double need = 1.5 * q.n + q.m / 16.0 + 64.0;
+    const double need = 3.0 * q.n + q.m / 8.0 + 64.0;
     sum_need += need;
     unsigned ptl = next_pow2((unsigned long long)(need * grow / ADDS_PAGE) + 8ull);
     if (ptl < 4) ptl = 4;
@@ -185,6 +197,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
     memset(&d, 0, sizeof d);
     d.row = q.row;
     d.edges = q.edges;
+    d.split = q.split;
     d.dist = q.dist;
     d.n = q.n;
     d.src = q.src;
@@ -193,7 +206,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
     d.shift0 = q.shift;
     d.graph_id = q.graph_id;
     E.qs_host[i] = d;
-    pt_words += (size_t)ADDS_NB << ptl;
+    pt_words += (size_t)2 * ADDS_NB << ptl;
     if (q.n > E.max_n) E.max_n = q.n;
   }
   unsigned long long pages = (unsigned long long)(sum_need * grow / ADDS_PAGE) + 2ull * ADDS_NB * E.nq + 64ull;
@@ -221,7 +234,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
   ALLOC(E.g, sizeof(GlobalCtl));
   ALLOC(E.qs, (size_t)E.nq * sizeof(QueryDesc));
   ALLOC(E.ctl, (size_t)E.nq * sizeof(QueryCtl));
-  ALLOC(E.slots, (size_t)E.nq * ADDS_NB * sizeof(SlotCtr));
+  ALLOC(E.slots, (size_t)E.nq * 2 * ADDS_NB * sizeof(SlotCtr));
   ALLOC(E.pt, pt_words * 8);
   ALLOC(E.reach, 16);
 #undef ALLOC
@@ -233,8 +246,8 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
   size_t off = 0;
   for (unsigned i = 0; i < E.nq; ++i) {
     E.qs_host[i].pt = E.pt + off;
-    off += (size_t)ADDS_NB << E.qs_host[i].ptn_log2;
-    E.qs_host[i].slots = E.slots + (size_t)i * ADDS_NB;
+    off += (size_t)2 * ADDS_NB << E.qs_host[i].ptn_log2;
+    E.qs_host[i].slots = E.slots + (size_t)i * 2 * ADDS_NB;
     E.qs_host[i].ctl = E.ctl + i;
   }
   int rc = engine_upload_queries(E, st);
@@ -244,7 +257,8 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 
 /* resolved knobs */
 struct Knobs {
-  int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt;
+  int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
+      light_heavy, block, greed;
   unsigned long long timeout_ns;
 };
 
@@ -253,9 +267,13 @@ static EngParams make_params(const Engine &E, const Knobs &k, unsigned single_sr
   memset(&P, 0, sizeof P);
   P.qs = E.qs;
   P.nq = E.nq;
+  const int blk = (k.block == 128 || k.block == 256 || k.block == 512) ? k.block : 256;
+  const int maxb = E.max_bps[block_index(blk)];
   int cps = k.ctas_per_sm;
-  if (cps <= 0 || cps > E.max_bps) cps = E.max_bps;
+  if (cps <= 0 || cps > maxb) cps = maxb;
   P.nctas = (unsigned)(cps * E.num_sms);
+  P.block = (unsigned)blk;
+  P.greed = (unsigned)std::max(0, std::min(k.greed, 12));
   P.g = E.g;
   P.pool = E.pool;
   P.pgen = E.pgen;
@@ -269,25 +287,39 @@ static EngParams make_params(const Engine &E, const Knobs &k, unsigned single_sr
   P.alloc_wait_ns = 200ull * 1000ull * 1000ull;
   if (P.alloc_wait_ns > k.timeout_ns) P.alloc_wait_ns = k.timeout_ns;
   P.window = (unsigned)std::max(1, std::min(k.window, ADDS_NB));
-  P.batch_max = (unsigned)std::max(1, std::min(k.batch_max, E.block));
+  P.batch_max = (unsigned)std::max(1, std::min(k.batch_max, blk));
   P.hub_threshold = (unsigned)std::max(k.hub_threshold, 64);
   P.hub_chunk = (unsigned)std::max(k.hub_chunk, 64);
+  if (P.hub_chunk > P.hub_threshold) P.hub_chunk = P.hub_threshold;
   P.strict_order = (unsigned)k.strict;
   P.adapt = (unsigned)k.adapt;
   P.is_float = E.flt ? 1u : 0u;
   P.single_src = single_src;
+  P.local_max = (unsigned)std::max(0, std::min(k.local_max, blk));
+  P.local_max_hungry = P.local_max / 8u;
   return P;
 }
 
-static int engine_enqueue(Engine &E, const EngParams &P, cudaStream_t st) {
+static int engine_enqueue(Engine &E, const EngParams &P, cudaStream_t st,
+                          cudaEvent_t k0 = nullptr, cudaEvent_t k1 = nullptr) {
+  /* under stream capture the records must be external nodes to stay
+   * usable for timing; outside capture the flag is not allowed */
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cs));
+  const unsigned fl = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
   CK(adds_engine_launch_init(P, E.max_n, st));
-  CK(adds_engine_launch_solve(P, st));
+  if (k0) CK(cudaEventRecordWithFlags(k0, st, fl));
+  CK(adds_engine_launch_solve(P, (int)P.block, st));
+  if (k1) CK(cudaEventRecordWithFlags(k1, st, fl));
   CK(cudaMemcpyAsync(E.g_host, E.g, sizeof(GlobalCtl), cudaMemcpyDeviceToHost, st));
   return ADDS_OK;
 }
 
 /* device error word -> ABI code (after the stream has been synchronised) */
 static int engine_status(const Engine &E) {
+  if (E.g_host->err)
+    snprintf(g_last_err, sizeof g_last_err, "device error %u at wait site %u", E.g_host->err,
+             E.g_host->err_where);
   switch (E.g_host->err) {
     case ADDS_DEV_OK: return ADDS_OK;
     case ADDS_DEV_OVERFLOW: return ADDS_ERR_WL_OVERFLOW;
@@ -305,6 +337,10 @@ static void fill_stats(const Engine &E, const EngParams &P, adds_stats *s) {
   s->pushes = g.st_pushes;
   s->batches = g.st_batches;
   s->hub_chunks = g.st_hub;
+  s->hub_stale = g.st_hub_stale;
+  s->local_batches = g.st_local;
+  s->heavy_lists = g.st_heavy;
+  for (int i = 0; i < 6; ++i) s->phase_cycles[i] = g.st_cyc[i];
   s->ctas = (int32_t)P.nctas;
 }
 
@@ -318,6 +354,10 @@ struct adds_graph {
   unsigned *row = nullptr;
   uint2 *edges = nullptr;
   unsigned *dist = nullptr;
+  uint2 *sedges = nullptr;     /* rows sorted by weight (light edges first)   */
+  unsigned *split = nullptr;   /* light-edge count per row for split_thr      */
+  unsigned split_thr = 0;
+  bool sorted_valid = false, split_valid = false;
   cudaStream_t stream = nullptr;
   uint32_t max_deg = 0;
   double avg_deg = 0, avg_w = 0;
@@ -330,6 +370,10 @@ struct adds_graph {
   Knobs last_knobs;
   EngParams last_params;
   int pending = 0; /* async solves enqueued since the last sync */
+  /* per-solve event ring: (start, kernel start, kernel end, end) */
+  static constexpr int kRing = 256;
+  cudaEvent_t ring[kRing][4] = {};
+  int ring_used = 0;
 };
 
 static int set_device(int dev) {
@@ -452,8 +496,13 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->row) cudaFree(g->row);
   if (g->edges) cudaFree(g->edges);
   if (g->dist) cudaFree(g->dist);
+  if (g->sedges) cudaFree(g->sedges);
+  if (g->split) cudaFree(g->split);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
+  for (int i = 0; i < adds_graph::kRing; ++i)
+    for (int j = 0; j < 4; ++j)
+      if (g->ring[i][j]) cudaEventDestroy(g->ring[i][j]);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -675,6 +724,7 @@ extern "C" int adds_graph_set_weights(adds_graph *g, const void *w) {
   if (tmp) cudaFree(tmp);
   cudaFree(bad);
   if (hb) return ADDS_ERR_INVALID;
+  g->sorted_valid = g->split_valid = false; /* the weight order changed */
   /* the weight sample feeds the automatic delta */
   double sw = 0;
   double *d_sw = nullptr;
@@ -739,26 +789,150 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   k->window = o->window > 0 ? o->window : (t->window > 0 ? t->window : 2);
   k->ctas_per_sm = o->ctas_per_sm > 0 ? o->ctas_per_sm : t->ctas_per_sm;
   k->batch_max = o->batch_max > 0 ? o->batch_max : (t->batch_max > 0 ? t->batch_max : 512);
-  k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : 16384);
-  k->hub_chunk = 4096;
+
   k->strict = o->strict_order >= 0 ? o->strict_order : (t->strict_order >= 0 ? t->strict_order : 1);
   k->adapt = o->adapt >= 0 ? o->adapt : (t->adapt >= 0 ? t->adapt : 0);
+  k->local_max = o->local_max >= 0 ? o->local_max : (t->local_max >= 0 ? t->local_max : 512);
+  k->light_heavy = o->light_heavy >= 0 ? o->light_heavy : (t->light_heavy >= 0 ? t->light_heavy : 1);
+  k->block = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 256);
+  k->greed = o->greed >= 0 ? o->greed : (t->greed >= 0 ? t->greed : 4);
+  k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : 16384);
+  k->hub_chunk = 4096;
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
 
 /* ------------------------------------------------------------------------ */
-/* plain solves                                                               */
-static int graph_engine(adds_graph *g, int shift, float scale) {
-  if (g->eng.nq == 1 && g->eng.qs_host[0].shift0 == (unsigned)shift && g->eng.qs_host[0].scale == scale)
+/* light/heavy support: a copy of the CSR with each row sorted by weight and,
+ * for the current bucket width, the number of light edges (w < delta) at the
+ * start of each row.  Heavy edges cannot land in the bucket their tail
+ * vertex is in, so they are relaxed once, after that bucket has settled. */
+__global__ void k_unzip(const uint2 *e, uint64_t m, uint32_t *w, uint32_t *d) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 x = e[i];
+    w[i] = x.y;
+    d[i] = x.x;
+  }
+}
+__global__ void k_zip(const uint32_t *w, const uint32_t *d, uint64_t m, uint2 *e) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    e[i] = make_uint2(d[i], w[i]);
+}
+__global__ void k_split(const unsigned *row, const uint2 *se, uint32_t n, unsigned thr,
+                        unsigned *split) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    unsigned lo = row[v], hi = row[v + 1];
+    const unsigned r0 = lo;
+    while (lo < hi) { /* first edge with weight >= thr */
+      const unsigned mid = lo + ((hi - lo) >> 1);
+      if (se[mid].y < thr) lo = mid + 1; else hi = mid;
+    }
+    split[v] = lo - r0;
+  }
+}
+
+static int graph_sorted(adds_graph *g) {
+  if (g->sorted_valid) return ADDS_OK;
+  const size_t m = g->m;
+  if (!g->sedges) {
+    CK(cudaMalloc(&g->sedges, (m ? m : 1) * sizeof(uint2)));
+    g->bytes += m * sizeof(uint2);
+  }
+  if (m == 0) {
+    g->sorted_valid = true;
     return ADDS_OK;
-  if (g->eng.nq == 1) { /* same sizing: only the descriptor changes */
-    g->eng.qs_host[0].shift0 = (unsigned)shift;
-    g->eng.qs_host[0].scale = scale;
+  }
+  if (m >= 0x7FFFFFFFull) return ADDS_ERR_UNSUPPORTED;
+  uint32_t *buf = nullptr;
+  CK(cudaMalloc(&buf, m * 16));
+  uint32_t *wk = buf, *dv = buf + m, *wk2 = buf + 2 * m, *dv2 = buf + 3 * m;
+  k_unzip<<<592, 256, 0, g->stream>>>(g->edges, m, wk, dv);
+  size_t tb = 0;
+  cub::DeviceSegmentedSort::SortPairs(nullptr, tb, wk, wk2, dv, dv2, (int)m, (int)g->n, g->row,
+                                      g->row + 1, g->stream);
+  void *tmp = nullptr;
+  cudaError_t e = cudaMalloc(&tmp, tb ? tb : 1);
+  if (e != cudaSuccess) {
+    cudaFree(buf);
+    return cuda_fail(e, "sort temp");
+  }
+  e = cub::DeviceSegmentedSort::SortPairs(tmp, tb, wk, wk2, dv, dv2, (int)m, (int)g->n, g->row,
+                                          g->row + 1, g->stream);
+  if (e == cudaSuccess) {
+    k_zip<<<592, 256, 0, g->stream>>>(wk2, dv2, m, g->sedges);
+    e = cudaStreamSynchronize(g->stream);
+  }
+  cudaFree(tmp);
+  cudaFree(buf);
+  if (e != cudaSuccess) return cuda_fail(e, "segmented sort");
+  g->sorted_valid = true;
+  g->split_valid = false;
+  return ADDS_OK;
+}
+
+/* light threshold in weight bits for bucket width 2^shift key units */
+static unsigned light_threshold(const adds_graph *g, int shift, float scale) {
+  if (g->wt == ADDS_I32) return shift >= 31 ? 0xFFFFFFFFu : (1u << shift);
+  const double dw = ldexp(1.0, shift) / (double)scale;
+  if (!(dw < 3.0e38)) return 0xFFFFFFFFu;
+  const float f = (float)dw;
+  unsigned b;
+  memcpy(&b, &f, 4);
+  return b;
+}
+
+static int graph_split(adds_graph *g, unsigned thr) {
+  int rc = graph_sorted(g);
+  if (rc) return rc;
+  if (g->split_valid && g->split_thr == thr) return ADDS_OK;
+  if (!g->split) {
+    CK(cudaMalloc(&g->split, ((size_t)g->n ? g->n : 1) * 4));
+    g->bytes += (size_t)g->n * 4;
+  }
+  k_split<<<592, 256, 0, g->stream>>>(g->row, g->sedges, g->n, thr, g->split);
+  CK(cudaStreamSynchronize(g->stream));
+  g->split_thr = thr;
+  g->split_valid = true;
+  return ADDS_OK;
+}
+
+/* edge array and light counts the engine should use for this graph */
+static int graph_layout(adds_graph *g, const Knobs &k, int shift, float scale,
+                        const uint2 **edges, const unsigned **split) {
+  if (!k.light_heavy) {
+    *edges = g->edges;
+    *split = nullptr;
+    return ADDS_OK;
+  }
+  const int rc = graph_split(g, light_threshold(g, shift, scale));
+  if (rc) return rc;
+  *edges = g->sedges;
+  *split = g->split;
+  return ADDS_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* plain solves                                                               */
+static int graph_engine(adds_graph *g, const Knobs &k, int shift, float scale) {
+  const uint2 *edges;
+  const unsigned *split;
+  int rc = graph_layout(g, k, shift, scale, &edges, &split);
+  if (rc) return rc;
+  if (g->eng.nq == 1) {
+    QueryDesc &d = g->eng.qs_host[0];
+    if (d.shift0 == (unsigned)shift && d.scale == scale && d.edges == edges && d.split == split)
+      return ADDS_OK;
+    /* same sizing: only the descriptor changes */
+    d.shift0 = (unsigned)shift;
+    d.scale = scale;
+    d.edges = edges;
+    d.split = split;
     return engine_upload_queries(g->eng, g->stream);
   }
   std::vector<EngQuery> qv(1);
-  qv[0] = EngQuery{g->row, g->edges, g->dist, g->n, g->m, 0u, scale, (unsigned)shift, 0u};
+  qv[0] = EngQuery{g->row, edges, split, g->dist, g->n, g->m, 0u, scale, (unsigned)shift, 0u};
   return engine_alloc(g->eng, g->device, g->wt == ADDS_F32, qv, g->grow, g->stream);
 }
 
@@ -766,23 +940,48 @@ static cudaStream_t pick_stream(const adds_graph *g, const adds_opts *o) {
   return (o && o->stream) ? (cudaStream_t)o->stream : g->stream;
 }
 
-/* Enqueues one solve; no host synchronisation. */
-static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts, bool timed) {
+/* Enqueues one solve; no host synchronisation.  Each solve records four
+ * events (start, solver start, solver end, end) in the graph's ring. */
+static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts) {
   int shift;
   float scale;
   Knobs k;
   resolve(g, opts, &k, &shift, &scale);
-  int rc = graph_engine(g, shift, scale);
+  int rc = graph_engine(g, k, shift, scale);
   if (rc) return rc;
   cudaStream_t st = pick_stream(g, opts);
   EngParams P = make_params(g->eng, k, src);
   g->last_knobs = k;
   g->last_params = P;
-  if (timed) CK(cudaEventRecord(g->ev0, st));
-  rc = engine_enqueue(g->eng, P, st);
+  if (g->ring_used == adds_graph::kRing) { /* ring full: fold into nothing */
+    CK(cudaStreamSynchronize(st));
+    g->ring_used = 0;
+  }
+  cudaEvent_t *ev = g->ring[g->ring_used];
+  for (int j = 0; j < 4; ++j)
+    if (!ev[j]) CK(cudaEventCreate(&ev[j]));
+  CK(cudaEventRecord(ev[0], st));
+  rc = engine_enqueue(g->eng, P, st, ev[1], ev[2]);
   if (rc) return rc;
-  if (timed) CK(cudaEventRecord(g->ev1, st));
+  CK(cudaEventRecord(ev[3], st));
+  ++g->ring_used;
   return ADDS_OK;
+}
+
+/* total and solver-kernel time of the solves in the ring (stream synced) */
+static void ring_times(adds_graph *g, double *ms, double *kms) {
+  double a = 0, b = 0;
+  for (int i = 0; i < g->ring_used; ++i) {
+    float x = 0, y = 0;
+    cudaEventElapsedTime(&x, g->ring[i][0], g->ring[i][3]);
+    cudaEventElapsedTime(&y, g->ring[i][1], g->ring[i][2]);
+    a += x;
+    b += y;
+  }
+  cudaGetLastError();
+  g->ring_used = 0;
+  *ms = a;
+  *kms = b;
 }
 
 extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds_opts *opts,
@@ -792,29 +991,33 @@ extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds
   if (rc) return rc;
   cudaStream_t st = pick_stream(g, opts);
   int retries = 0;
+  CK(cudaStreamSynchronize(st));
+  g->ring_used = 0;
   for (;;) {
-    rc = sssp_enqueue(g, src, opts, true);
+    rc = sssp_enqueue(g, src, opts);
     if (rc) return rc;
     CK(cudaStreamSynchronize(st));
     rc = engine_status(g->eng);
     if (rc == ADDS_ERR_WL_OVERFLOW && retries < 4) {
       ++retries;
       g->grow *= 2;
-      g->eng.nq = 0; /* force re-allocation at the larger size */
-      engine_free(g->eng);
+      engine_free(g->eng); /* re-allocated at the larger size on the rerun */
+      g->ring_used = 0;
       continue;
     }
     if (rc) {
       engine_full_reset(g->eng, st);
+      g->ring_used = 0;
       return rc;
     }
     break;
   }
+  double ms = 0, kms = 0;
+  ring_times(g, &ms, &kms);
   if (stats) {
     memset(stats, 0, sizeof *stats);
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
     stats->ms = ms;
+    stats->kernel_ms = kms;
     fill_stats(g->eng, g->last_params, stats);
     stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
     stats->retries = retries;
@@ -830,7 +1033,7 @@ extern "C" int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opt
   if (!g || src >= g->n) return ADDS_ERR_INVALID;
   int rc = set_device(g->device);
   if (rc) return rc;
-  rc = sssp_enqueue(g, src, opts, false);
+  rc = sssp_enqueue(g, src, opts);
   if (!rc) ++g->pending;
   return rc;
 }
@@ -840,6 +1043,8 @@ extern "C" int adds_graph_sync(adds_graph *g, adds_stats *stats) {
   int rc = set_device(g->device);
   if (rc) return rc;
   CK(cudaStreamSynchronize(g->stream));
+  double ms = 0, kms = 0;
+  ring_times(g, &ms, &kms);
   if (g->eng.nq == 0) return ADDS_OK;
   rc = engine_status(g->eng);
   g->pending = 0;
@@ -849,6 +1054,8 @@ extern "C" int adds_graph_sync(adds_graph *g, adds_stats *stats) {
   }
   if (stats) {
     memset(stats, 0, sizeof *stats);
+    stats->ms = ms;
+    stats->kernel_ms = kms;
     fill_stats(g->eng, g->last_params, stats);
     stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
   }
@@ -902,7 +1109,7 @@ struct adds_batch {
   std::vector<float> scales;
   cudaGraphExec_t exec = nullptr;
   bool captured = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
   EngParams P;
   void *adj = nullptr; /* backward scratch (adjoint.cu) */
 };
@@ -911,7 +1118,11 @@ static int batch_engine(adds_batch *b) {
   std::vector<EngQuery> qv(b->qgraph.size());
   for (size_t i = 0; i < qv.size(); ++i) {
     adds_graph *g = b->qgraph[i];
-    qv[i] = EngQuery{g->row, g->edges, b->dist_all + b->dist_off[i], g->n, g->m, b->srcs[i],
+    const uint2 *edges;
+    const unsigned *split;
+    const int rc = graph_layout(g, b->kn, b->shifts[i], b->scales[i], &edges, &split);
+    if (rc) return rc;
+    qv[i] = EngQuery{g->row, edges, split, b->dist_all + b->dist_off[i], g->n, g->m, b->srcs[i],
                      b->scales[i], (unsigned)b->shifts[i], b->qgid[i]};
   }
   if (b->exec) {
@@ -971,7 +1182,8 @@ extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs
     if (i == 0) b->kn = k;
   }
   if (cudaMalloc(&b->dist_all, tot * 4) != cudaSuccess ||
-      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+      cudaEventCreate(&b->k0) != cudaSuccess || cudaEventCreate(&b->k1) != cudaSuccess) {
     cudaGetLastError();
     adds_batch_free(b);
     return ADDS_ERR_OOM;
@@ -994,6 +1206,8 @@ extern "C" void adds_batch_free(adds_batch *b) {
   if (b->dist_all) cudaFree(b->dist_all);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->k0) cudaEventDestroy(b->k0);
+  if (b->k1) cudaEventDestroy(b->k1);
   if (b->adj) adds_adjoint_free(b->adj);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -1003,7 +1217,7 @@ extern "C" void adds_batch_free(adds_batch *b) {
 static int batch_capture(adds_batch *b) {
   cudaGraph_t gr = nullptr;
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = engine_enqueue(b->eng, b->P, b->stream);
+  int rc = engine_enqueue(b->eng, b->P, b->stream, b->k0, b->k1);
   cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
   if (rc || e != cudaSuccess) {
     if (gr) cudaGraphDestroy(gr);
@@ -1038,9 +1252,11 @@ extern "C" int adds_batch_sync(adds_batch *b, adds_stats *stats) {
   if (rc) return rc;
   if (stats) {
     memset(stats, 0, sizeof *stats);
-    float ms = 0;
+    float ms = 0, kms = 0;
     CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    CK(cudaEventElapsedTime(&kms, b->k0, b->k1));
     stats->ms = ms;
+    stats->kernel_ms = kms;
     fill_stats(b->eng, b->P, stats);
     stats->delta_shift = b->shifts.empty() ? 0 : b->shifts[0];
   }
@@ -1170,6 +1386,10 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   cur.batch_max = k.batch_max;
   cur.hub_threshold = k.hub_threshold;
   cur.strict_order = k.strict;
+  cur.local_max = k.local_max;
+  cur.light_heavy = k.light_heavy;
+  cur.block_threads = k.block;
+  cur.greed = k.greed;
   double bm = time_solves(g, srcs, ns, &cur);
   auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
     for (int v : vals) {
@@ -1189,12 +1409,16 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   try_field(&adds_opts::delta_shift, shifts);
   try_field(&adds_opts::window, {1, 2, 3, 4, 8});
   try_field(&adds_opts::batch_max, {64, 128, 256, 512});
-  try_field(&adds_opts::hub_threshold, {2048, 4096, 16384, 65536});
-  int maxb = g->eng.max_bps;
+  try_field(&adds_opts::hub_threshold, {4096, 16384, 65536});
+  try_field(&adds_opts::block_threads, {128, 256, 512});
+  try_field(&adds_opts::greed, {0, 2, 4, 8});
+  int maxb = g->eng.max_bps[block_index(cur.block_threads > 0 ? cur.block_threads : 256)];
   std::vector<int> cps;
   for (int c = 1; c <= maxb; ++c) cps.push_back(c);
   try_field(&adds_opts::ctas_per_sm, cps);
   try_field(&adds_opts::strict_order, {0, 1});
+  try_field(&adds_opts::local_max, {0, 64, 256, 512});
+  try_field(&adds_opts::light_heavy, {0, 1});
   if (cur.delta_shift != s0) { /* second look around the new delta */
     std::vector<int> s2;
     for (int d = -1; d <= 1; ++d)

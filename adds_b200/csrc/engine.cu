@@ -140,14 +140,21 @@ __device__ __forceinline__ unsigned long long *pt_cell(const QueryDesc &d, unsig
 }
 
 /* Waits until virtual page vp of slot s is mapped (translate_write_ptr,
- * wl.h:1874-1900, resolved from an HBM page table instead of a smem cache). */
+ * wl.h:1874-1900, resolved from an HBM page table; `cvp`/`cpi` are the
+ * CTA's cached mapping for the slot, checked and refreshed here). */
 __device__ unsigned pt_wait(const EngParams &P, const QueryDesc &d, unsigned s,
-                            unsigned long long vp, unsigned long long deadline) {
+                            unsigned long long vp, unsigned long long deadline,
+                            unsigned long long *cvp, unsigned *cpi) {
+  if (*cvp == vp) return *cpi;
   unsigned long long *cell = pt_cell(d, s, vp);
   Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
   for (;;) {
     const unsigned long long e = ld_rlx64(cell);
-    if ((unsigned)e == (unsigned)vp) return (unsigned)(e >> 32);
+    if ((unsigned)e == (unsigned)vp) {
+      *cvp = vp;
+      *cpi = (unsigned)(e >> 32);
+      return *cpi;
+    }
     if (!w.spin(P.g, W_PT)) return PI_BAD;
   }
 }
@@ -158,7 +165,8 @@ __device__ unsigned pt_wait(const EngParams &P, const QueryDesc &d, unsigned s,
  * reservation + translate (wl.h:1902-1928). */
 __device__ bool slot_reserve(const EngParams &P, const QueryDesc &d, unsigned s,
                              unsigned c, unsigned long long deadline,
-                             unsigned long long *pbase, unsigned *pp0, unsigned *pp1) {
+                             unsigned long long *pbase, unsigned *pp0, unsigned *pp1,
+                             unsigned long long *cvp, unsigned *cpi) {
   SlotCtr *sc = d.slots + s;
   const unsigned long long base = atomicAdd(&sc->tail, (unsigned long long)c);
   *pbase = base;
@@ -177,8 +185,10 @@ __device__ bool slot_reserve(const EngParams &P, const QueryDesc &d, unsigned s,
       pi = alloc_page(P, deadline);
       if (pi == PI_BAD) return false;
       st_rlx64(pt_cell(d, s, vp), ((unsigned long long)pi << 32) | (unsigned)vp);
+      *cvp = vp;
+      *cpi = pi;
     } else {
-      pi = pt_wait(P, d, s, vp, deadline);
+      pi = pt_wait(P, d, s, vp, deadline, cvp, cpi);
       if (pi == PI_BAD) return false;
     }
     if (vp == vp0) *pp0 = pi; else *pp1 = pi;
@@ -213,6 +223,8 @@ __device__ __forceinline__ unsigned bucket_slot(unsigned key, unsigned shift,
 
 /* ------------------------------------------------------------------------ */
 /* shared memory of one CTA                                                   */
+#define NSLOT (2 * ADDS_NB) /* light buckets [0, NB), heavy lists [NB, 2NB) */
+
 template <int BLOCK>
 struct Smem {
   static constexpr int U = 4;               /* edges per thread per round    */
@@ -220,14 +232,17 @@ struct Smem {
   unsigned it_rb[BLOCK];                    /* first edge of each item       */
   unsigned it_du[BLOCK];                    /* distance used for the item    */
   unsigned it_off[BLOCK];                   /* exclusive scan of degrees     */
+  unsigned loc_v[BLOCK];                    /* own pushes kept for next batch */
+  unsigned loc_d[BLOCK];
   unsigned pb_v[SB];
   unsigned pb_d[SB];
   unsigned short pb_rank[SB];
   unsigned char pb_s[SB];
-  unsigned long long bbase[ADDS_NB];
-  unsigned bp0[ADDS_NB];
-  unsigned bp1[ADDS_NB];
-  unsigned hist[ADDS_NB];
+  unsigned long long bbase[NSLOT];
+  unsigned bp0[NSLOT];
+  unsigned bp1[NSLOT];
+  unsigned hist[NSLOT];
+  unsigned gcnt[NSLOT];                     /* per-slot entries sent to HBM  */
   unsigned wsum[BLOCK / 32];
   /* batch descriptor written by the acquiring warp */
   unsigned long long h;
@@ -235,16 +250,48 @@ struct Smem {
   unsigned pi0, pi1;
   unsigned base_b, base_key, shift;
   unsigned pcnt, total_edges, hub_chunks;
-  unsigned cur_q, idle;
+  unsigned cur_q, idle, hungry;
+  unsigned loc_k, loc_slot, keep_slot;
+  unsigned hub_u, ptc_q;
+  /* page-table cache: last (virtual page -> page info) seen per slot of
+   * query ptc_q.  A claimed or reserved entry keeps its page mapped, so a
+   * hit on the same virtual page is always current. */
+  unsigned long long ptc_vp[NSLOT];
+  unsigned ptc_pi[NSLOT];
 };
 
-enum : unsigned { ST_WORK = 0, ST_HUB = 1, ST_IDLE = 2, ST_EXIT = 3 };
+enum : unsigned { ST_WORK = 0, ST_HUB = 1, ST_IDLE = 2, ST_EXIT = 3, ST_LOCAL = 4, ST_HEAVY = 5 };
+
+/* claim up to ~avail/nctas entries of one slot: inflight first (so the
+ * bucket is never seen empty and drained while entries are held), then the
+ * avail count, then the head index.  Returns the count, 0 if none. */
+__device__ __forceinline__ unsigned claim(SlotCtr *sc, long long av, const EngParams &P,
+                                          unsigned long long *h0) {
+  const long long share = (long long)((P.nctas >> P.greed) ? (P.nctas >> P.greed) : 1u);
+  long long want = (av + share - 1) / share;
+  if (want > (long long)P.batch_max) want = P.batch_max;
+  if (want < 1) want = 1;
+  atomicAdd(&sc->inflight, (unsigned long long)want);
+  const long long old =
+      (long long)atomicAdd((unsigned long long *)&sc->avail, (unsigned long long)(-want));
+  long long got = old < want ? old : want;
+  if (got < 0) got = 0;
+  if (got < want) {
+    atomicAdd((unsigned long long *)&sc->avail, (unsigned long long)(want - got));
+    atomicAdd(&sc->inflight, (unsigned long long)(got - want));
+  }
+  if (got > 0) *h0 = atomicAdd(&sc->head, (unsigned long long)got);
+  return (unsigned)got;
+}
 
 /* ------------------------------------------------------------------------ */
 /* Acquire a batch (warp 0).  Replaces the assign manager + get_global
- * mailbox handshake (wl.h:851-1527, 1698-1853): the CTA itself pops from
- * the lowest non-empty bucket in the window with a CAS on the slot head and
- * retires the lowest bucket when it is empty and drained. */
+ * mailbox handshake (wl.h:851-1527, 1698-1853).  Per query, the lowest live
+ * bucket goes through two phases: L, its vertices are popped and their
+ * light edges relaxed (buckets up to window-1 above it may run too), and
+ * H, once its light queue is empty and drained, the heavy-edge lists of the
+ * vertices it settled are expanded.  When both are empty and drained the
+ * bucket retires and the next non-empty one becomes the base. */
 template <int BLOCK>
 __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
                         unsigned long long deadline) {
@@ -279,23 +326,21 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
         }
         if (ok) {
           const unsigned *hp = reinterpret_cast<const unsigned *>(P.hub + (ticket & mask));
-          HubChunk c;
-          c.q = __ldcg(hp);
-          c.du = __ldcg(hp + 1);
-          c.eb = __ldcg(hp + 2);
-          c.ee = __ldcg(hp + 3);
+          const unsigned cq = __ldcg(hp), cu = __ldcg(hp + 1), cdu = __ldcg(hp + 2),
+                         ceb = __ldcg(hp + 3), cee = __ldcg(hp + 4);
           __threadfence();
           st_rel32(seq, (unsigned)(ticket + (1ull << ADDS_HUB_RING_LOG2)));
           S.status = ST_HUB;
-          S.q = c.q;
+          S.q = cq;
           S.k = 1;
-          S.it_rb[0] = c.eb;
-          S.it_du[0] = c.du;
+          S.hub_u = cu;
+          S.it_rb[0] = ceb;
+          S.it_du[0] = cdu;
           S.it_off[0] = 0;
-          S.total_edges = c.ee - c.eb;
-          const QueryCtl *ctl = P.qs[c.q].ctl;
+          S.total_edges = cee - ceb;
+          const QueryCtl *ctl = P.qs[cq].ctl;
           const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
-          S.base_b = (unsigned)ctrl;
+          S.base_b = (unsigned)ctrl & 0x7FFFFFFFu;
           S.base_key = (unsigned)(ctrl >> 32);
           S.shift = ld_rlx32(&ctl->shift);
         } else {
@@ -313,72 +358,95 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
     QueryCtl *ctl = d.ctl;
     if (ld_rlx32(&ctl->done) != 0u) continue;
     const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
-    const unsigned base_b = (unsigned)ctrl;
+    const unsigned base_b = (unsigned)ctrl & 0x7FFFFFFFu;
+    const bool phase_h = ((unsigned)ctrl & ADDS_PHASE_H) != 0u;
     const unsigned base_key = (unsigned)(ctrl >> 32);
     const unsigned s = (base_b + lane) & (ADDS_NB - 1u);
-    SlotCtr *sc = d.slots + s;
-    const unsigned long long h = ld_rlx64(&sc->head);
-    const unsigned long long tl = ld_rlx64(&sc->tail);
-    const unsigned mask = __ballot_sync(0xFFFFFFFFu, tl > h);
-    if (mask == 0u) {
+    SlotCtr *lsc = d.slots + s;
+    SlotCtr *hsc = d.slots + ADDS_NB + s;
+    const unsigned long long lh = ld_rlx64(&lsc->head), lt = ld_rlx64(&lsc->tail);
+    const long long lav = (long long)ld_rlx64((const unsigned long long *)&lsc->avail);
+    const unsigned long long hh = ld_rlx64(&hsc->head), ht = ld_rlx64(&hsc->tail);
+    const long long hav = (long long)ld_rlx64((const unsigned long long *)&hsc->avail);
+    const unsigned lmask = __ballot_sync(0xFFFFFFFFu, lt > lh);
+    const unsigned lamask = __ballot_sync(0xFFFFFFFFu, lav > 0);
+    const unsigned hmask = __ballot_sync(0xFFFFFFFFu, ht > hh);
+    const unsigned hamask = __ballot_sync(0xFFFFFFFFu, hav > 0);
+    if ((lmask | hmask) == 0u) {
       if (lane == 0 && ld_rlx32(&ctl->live) == 0u) {
         if (atomicCAS(&ctl->done, 0u, 1u) == 0u) atomicSub(&g->remaining, 1u);
       }
       continue;
     }
-    unsigned first = __ffs(mask) - 1u;
-    if (first > 0u) {
-      /* lowest bucket is empty: retire it (and the empty ones after it)
-       * unless strict ordering says its popped entries are still running */
-      const unsigned long long infl0 =
-          __shfl_sync(0xFFFFFFFFu, ld_rlx64(&sc->inflight), 0);
-      const bool drained = (P.strict_order == 0u) || (infl0 == 0ull);
-      if (drained) {
-        if (lane == 0) {
-          const unsigned long long nc =
-              ((unsigned long long)(base_key + first) << 32) | (base_b + first);
-          atomicCAS(&ctl->ctrl, ctrl, nc);
-        }
-      } else if (first >= P.window) {
-        continue; /* only work beyond the window: wait for the lowest bucket */
-      }
-    }
-    /* pop from slot base+first */
-    unsigned want = 0;
-    unsigned long long got = ~0ull;
-    if (lane == first) {
-      unsigned long long hh = h;
-      for (int r = 0; r < 4; ++r) {
-        const unsigned long long avail = tl - hh;
-        if (tl <= hh) break;
-        unsigned long long w = (avail + P.nctas - 1ull) / P.nctas;
-        if (w > P.batch_max) w = P.batch_max;
-        if (w == 0ull) w = 1ull;
-        const unsigned long long prev = atomicCAS(&sc->head, hh, hh + w);
-        if (prev == hh) { got = hh; want = (unsigned)w; break; }
-        hh = prev;
-      }
-      if (got != ~0ull) atomicAdd(&sc->inflight, (unsigned long long)want);
-    }
-    got = __shfl_sync(0xFFFFFFFFu, got, first);
-    want = __shfl_sync(0xFFFFFFFFu, want, first);
-    if (got == ~0ull) continue;
+    unsigned long long li = 0, hi = 0;
     if (lane == 0) {
-      const unsigned long long vp0 = got >> ADDS_PAGE_LOG2;
-      const unsigned long long vp1 = (got + want - 1ull) >> ADDS_PAGE_LOG2;
-      const unsigned pi0 = pt_wait(P, d, (base_b + first) & (ADDS_NB - 1u), vp0, deadline);
+      li = ld_rlx64(&lsc->inflight);
+      hi = ld_rlx64(&hsc->inflight);
+    }
+    li = __shfl_sync(0xFFFFFFFFu, li, 0);
+    hi = __shfl_sync(0xFFFFFFFFu, hi, 0);
+    const bool strict = P.strict_order != 0u;
+    const bool l_done = !(lmask & 1u) && (!strict || li == 0ull);
+    const bool h_done = !(hmask & 1u) && (!strict || hi == 0ull);
+    /* base-bucket state machine */
+    unsigned eff = 0;      /* base after our transition, relative to base_b */
+    bool eff_h = phase_h;
+    unsigned long long nc = ctrl;
+    if (l_done) {
+      if (h_done) {
+        /* retire: the next bucket with light entries or a heavy list (a
+         * bucket above the base may have finished its light phase inside
+         * the window and left only its heavy list), in phase L */
+        const unsigned ahead = (lmask | hmask) & ~1u;
+        if (ahead) {
+          eff = __ffs(ahead) - 1u;
+          eff_h = false;
+          nc = ((unsigned long long)(base_key + eff) << 32) | ((base_b + eff) & 0x7FFFFFFFu);
+        }
+      } else if (!phase_h) { /* light phase over: expand the heavy lists */
+        eff_h = true;
+        nc = ((unsigned long long)base_key << 32) | base_b | ADDS_PHASE_H;
+      }
+    }
+    if (nc != ctrl && lane == 0) atomicCAS(&ctl->ctrl, ctrl, nc);
+    /* claim: heavy list of a base in phase H (or stale lists outside the
+     * window), else the lowest light bucket inside the window */
+    const unsigned win = P.window;
+    const unsigned wmask_l = (eff + win >= 32u) ? (0xFFFFFFFFu << eff)
+                                                : (((1u << win) - 1u) << eff);
+    /* heavy lists outside the active window belong to settled buckets */
+    unsigned hcand = hamask & ~wmask_l;
+    if (eff_h && eff == 0u) hcand |= hamask & 1u;  /* the base's heavy lists  */
+    const unsigned lcand = lamask & wmask_l;
+    bool heavy = hcand != 0u;
+    const unsigned j = heavy ? (__ffs(hcand) - 1u) : (lcand ? __ffs(lcand) - 1u : 32u);
+    if (j == 32u) continue;
+    unsigned got = 0;
+    unsigned long long h0 = 0;
+    if (lane == j) got = claim(heavy ? hsc : lsc, heavy ? hav : lav, P, &h0);
+    got = __shfl_sync(0xFFFFFFFFu, got, j);
+    h0 = __shfl_sync(0xFFFFFFFFu, h0, j);
+    if (got == 0u) continue;
+    if (lane == 0) {
+      const unsigned sid = ((base_b + j) & (ADDS_NB - 1u)) + (heavy ? ADDS_NB : 0u);
+      const unsigned long long vp0 = h0 >> ADDS_PAGE_LOG2;
+      const unsigned long long vp1 = (h0 + got - 1ull) >> ADDS_PAGE_LOG2;
+      if (S.ptc_q != q) { /* cache belongs to another query */
+        for (int i = 0; i < NSLOT; ++i) S.ptc_vp[i] = ~0ull;
+        S.ptc_q = q;
+      }
+      const unsigned pi0 = pt_wait(P, d, sid, vp0, deadline, &S.ptc_vp[sid], &S.ptc_pi[sid]);
       const unsigned pi1 = (vp1 == vp0) ? pi0
-                           : pt_wait(P, d, (base_b + first) & (ADDS_NB - 1u), vp1, deadline);
-      S.status = ST_WORK;
+                           : pt_wait(P, d, sid, vp1, deadline, &S.ptc_vp[sid], &S.ptc_pi[sid]);
+      S.status = heavy ? ST_HEAVY : ST_WORK;
       S.q = q;
-      S.slot = (base_b + first) & (ADDS_NB - 1u);
-      S.h = got;
-      S.k = want;
+      S.slot = sid;
+      S.h = h0;
+      S.k = got;
       S.pi0 = pi0;
       S.pi1 = pi1;
-      const unsigned long long c2 = ld_rlx64(&ctl->ctrl);
-      S.base_b = (unsigned)c2;
-      S.base_key = (unsigned)(c2 >> 32);
+      S.base_b = (base_b + eff) & 0x7FFFFFFFu;
+      S.base_key = base_key + eff;
       S.shift = ld_rlx32(&ctl->shift);
       S.cur_q = q;
     }
@@ -391,47 +459,101 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
 }
 
 /* ------------------------------------------------------------------------ */
-/* Flush staged pushes: counting sort by bucket slot in shared memory, one
- * tail reservation per non-empty slot, then the entry stores.  Replaces the
- * per-warp match_any + atomicAdd + st.cg + __threadfence + write_done update
- * of push_work (wl.h:1902-1928). */
+/* Flush staged pushes: counting sort by slot (light buckets and heavy lists)
+ * in shared memory.  With `keep`, the entries of the lowest light bucket
+ * inside the window (up to local_max) stay in shared memory as this CTA's
+ * next batch, so a wavefront advances without a round trip through HBM.
+ * Every other slot gets one tail reservation and the entry stores; its
+ * avail count is raised after the stores.  Replaces the per-warp match_any
+ * + atomicAdd + st.cg + __threadfence + write_done update of push_work
+ * (wl.h:1902-1928). */
 template <int BLOCK>
 __device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
-                      unsigned long long deadline, unsigned long long &st_pushes) {
+                      unsigned long long deadline, unsigned long long &st_pushes, bool keep) {
   const unsigned tid = threadIdx.x;
   const unsigned cnt = S.pcnt;
   if (cnt == 0u) return; /* uniform: read after a barrier */
-  if (tid < ADDS_NB) S.hist[tid] = 0u;
+  const unsigned qd = (unsigned)(&d - P.qs);
+  const bool stale_cache = S.ptc_q != qd; /* uniform: read after a barrier */
+  if (tid < NSLOT) {
+    S.hist[tid] = 0u;
+    if (stale_cache) S.ptc_vp[tid] = ~0ull;
+  }
   __syncthreads();
+  if (tid == 0u) S.ptc_q = qd;
   for (unsigned i = tid; i < cnt; i += BLOCK)
     S.pb_rank[i] = (unsigned short)atomicAdd(&S.hist[S.pb_s[i]], 1u);
   __syncthreads();
-  if (tid < 32u) {
+  if (tid < 32u) { /* warp 0: light buckets, local keep, live count */
     const unsigned c = S.hist[tid];
+    const unsigned nz = __ballot_sync(0xFFFFFFFFu, c != 0u);
+    unsigned ks = 0xFFFFFFFFu, kn = 0u;
+    if (keep && nz) {
+      const unsigned sh = S.base_b & 31u; /* bit r of rot = slot base_b + r */
+      const unsigned rot = sh ? ((nz >> sh) | (nz << (32u - sh))) : nz;
+      const unsigned r = __ffs(rot) - 1u;
+      if (r < P.window) {
+        ks = (S.base_b + r) & (ADDS_NB - 1u);
+        const unsigned lmax = ld_rlx32(&P.g->hungry) ? P.local_max_hungry : P.local_max;
+        kn = min(min(__shfl_sync(0xFFFFFFFFu, c, ks), lmax), (unsigned)BLOCK);
+      }
+    }
     if (tid == 0u) {
-      atomicAdd(&d.ctl->live, cnt); /* count before the entries are visible */
+      atomicAdd(&d.ctl->live, cnt); /* count before any entry is visible */
       __threadfence();
       st_pushes += cnt;
+      S.keep_slot = kn ? ks : 0xFFFFFFFFu;
+      S.loc_k = kn;
+      S.loc_slot = ks;
     }
     __syncwarp();
-    if (c != 0u) {
+    const unsigned cg = c - ((tid == ks) ? kn : 0u);
+    S.gcnt[tid] = cg;
+    if (tid == ks && kn) atomicAdd(&d.slots[ks].inflight, (unsigned long long)kn);
+    if (cg != 0u) {
       unsigned long long b;
       unsigned p0, p1;
-      slot_reserve(P, d, tid, c, deadline, &b, &p0, &p1);
+      slot_reserve(P, d, tid, cg, deadline, &b, &p0, &p1, &S.ptc_vp[tid], &S.ptc_pi[tid]);
       S.bbase[tid] = b;
       S.bp0[tid] = p0;
       S.bp1[tid] = p1;
     }
+  } else if (tid < 64u) { /* warp 1: heavy lists */
+    const unsigned sl = tid; /* NB + lane */
+    const unsigned c = S.hist[sl];
+    S.gcnt[sl] = c;
+    if (c != 0u) {
+      unsigned long long b;
+      unsigned p0, p1;
+      slot_reserve(P, d, sl, c, deadline, &b, &p0, &p1, &S.ptc_vp[sl], &S.ptc_pi[sl]);
+      S.bbase[sl] = b;
+      S.bp0[sl] = p0;
+      S.bp1[sl] = p1;
+    }
   }
   __syncthreads();
+  const unsigned ks = S.keep_slot, kn = S.loc_k;
   for (unsigned i = tid; i < cnt; i += BLOCK) {
     const unsigned s = S.pb_s[i];
+    const unsigned r = S.pb_rank[i];
+    if (s == ks && r < kn) {
+      S.loc_v[r] = S.pb_v[i];
+      S.loc_d[r] = S.pb_d[i];
+      continue;
+    }
     const unsigned long long b = S.bbase[s];
-    const unsigned long long idx = b + S.pb_rank[i];
+    const unsigned long long idx = b + r - (s == ks ? kn : 0u);
     const unsigned pi = ((idx >> ADDS_PAGE_LOG2) == (b >> ADDS_PAGE_LOG2)) ? S.bp0[s] : S.bp1[s];
     if (pi != PI_BAD) st_rlx64(entry_ptr(P, pi, idx), make_entry(S.pb_v[i], S.pb_d[i], pi));
   }
+  /* the entry stores of the whole CTA are ordered before the avail
+   * increments by the barrier plus one (cumulative) fence per raising
+   * thread; a popper that still sees an old entry waits on its phase bit */
   __syncthreads();
+  if (tid < NSLOT && S.gcnt[tid] != 0u) {
+    __threadfence();
+    atomicAdd((unsigned long long *)&d.slots[tid].avail, (unsigned long long)S.gcnt[tid]);
+  }
   if (tid == 0u) S.pcnt = 0u;
   __syncthreads();
 }
@@ -464,10 +586,22 @@ __device__ __forceinline__ unsigned block_exscan(Smem<BLOCK> &S, unsigned x, uns
   return S.wsum[warp] + incl - x;
 }
 
+/* stage one push in shared memory (warp-aggregated slot reservation) */
+template <int BLOCK>
+__device__ __forceinline__ void stage(Smem<BLOCK> &S, unsigned v, unsigned dd, unsigned slot) {
+  cg::coalesced_group grp = cg::coalesced_threads();
+  unsigned pos = 0;
+  if (grp.thread_rank() == 0) pos = atomicAdd(&S.pcnt, grp.size());
+  pos = grp.shfl(pos, 0) + grp.thread_rank();
+  S.pb_v[pos] = v;
+  S.pb_d[pos] = dd;
+  S.pb_s[pos] = (unsigned char)slot;
+}
+
 /* ------------------------------------------------------------------------ */
 /* the persistent solver                                                      */
 template <bool FLT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<BLOCK> &S = *reinterpret_cast<Smem<BLOCK> *>(smem_raw);
   constexpr int U = Smem<BLOCK>::U;
@@ -476,68 +610,126 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
   const unsigned long long deadline = gtimer() + P.timeout_ns;
 
   unsigned long long st_items = 0, st_stale = 0, st_edges = 0, st_pushes = 0,
-                     st_batches = 0, st_hub = 0;
+                     st_batches = 0, st_hub = 0, st_local = 0, st_hub_stale = 0,
+                     st_heavy = 0;
+  /* per-phase SM cycle counts (thread 0's view; every phase ends at a
+   * barrier, so thread 0 sees the CTA's time) */
+  unsigned long long cy_acq = 0, cy_load = 0, cy_edge = 0, cy_flush = 0, cy_idle = 0;
+  const long long cy_start = clock64();
+  long long cy_mark = cy_start;
+#define CY_LAP(acc)                     \
+  do {                                  \
+    const long long _n = clock64();     \
+    acc += (unsigned long long)(_n - cy_mark); \
+    cy_mark = _n;                       \
+  } while (0)
   if (tid == 0) {
     S.cur_q = blockIdx.x % P.nq;
     S.pcnt = 0;
     S.idle = 0;
+    S.hungry = 0;
     S.hub_chunks = 0;
+    S.loc_k = 0;
+    S.q = S.cur_q;
+    S.ptc_q = 0xFFFFFFFFu;
   }
+  if (tid < NSLOT) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
 
   for (;;) {
-    if (tid < 32) acquire<BLOCK>(P, S, deadline);
+    if (S.loc_k == 0u) { /* uniform: read after a barrier */
+      if (tid < 32) acquire<BLOCK>(P, S, deadline);
+    } else if (tid == 0) {
+      /* next batch = the entries this CTA kept from its own last flush */
+      S.status = ST_LOCAL;
+      S.k = S.loc_k;
+      S.slot = S.loc_slot;
+      const QueryCtl *ctl = P.qs[S.q].ctl;
+      const unsigned long long c2 = ld_rlx64(&ctl->ctrl);
+      S.base_b = (unsigned)c2 & 0x7FFFFFFFu;
+      S.base_key = (unsigned)(c2 >> 32);
+      S.shift = ld_rlx32(&ctl->shift);
+    }
     __syncthreads();
     const unsigned status = S.status;
+    if (status == ST_IDLE || status == ST_EXIT) CY_LAP(cy_idle); else CY_LAP(cy_acq);
     if (status == ST_EXIT) break;
     if (status == ST_IDLE) {
       if (tid == 0) {
         const unsigned n = ++S.idle;
+        if (!S.hungry) {
+          S.hungry = 1;
+          atomicAdd(&P.g->hungry, 1u);
+        }
         if (gtimer() > deadline) raise_err(P.g, ADDS_DEV_TIMEOUT, W_IDLE);
         __nanosleep(n < 8 ? 100 : (n < 64 ? 400 : 1000));
       }
       __syncthreads();
+      CY_LAP(cy_idle);
       continue;
     }
-    if (tid == 0) S.idle = 0;
+    if (tid == 0) {
+      S.idle = 0;
+      if (S.hungry) {
+        S.hungry = 0;
+        atomicSub(&P.g->hungry, 1u);
+      }
+    }
     const unsigned q = S.q;
     const QueryDesc &d = P.qs[q];
     const unsigned *__restrict__ row = d.row;
     const uint2 *__restrict__ edges = d.edges;
+    const unsigned *__restrict__ split = d.split;
     unsigned *dist = d.dist;
     const float scale = d.scale;
     const unsigned shift = S.shift, base_b = S.base_b, base_key = S.base_key;
     unsigned k = 1;
 
-    if (status == ST_WORK) {
+    if (status != ST_HUB) {
       k = S.k;
       const unsigned long long h = S.h;
+      const unsigned myslot = S.slot;
       unsigned deg = 0, rb = 0, dp = 0, chunks = 0;
       if (tid < k) {
-        const unsigned long long idx = h + tid;
-        const unsigned pi = ((idx >> ADDS_PAGE_LOG2) == (h >> ADDS_PAGE_LOG2)) ? S.pi0 : S.pi1;
-        bool ok = pi != PI_BAD;
-        unsigned long long e = 0;
-        if (ok) {
-          const unsigned long long *ep = entry_ptr(P, pi, idx);
-          Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
-          e = ld_rlx64(ep);
-          while (((unsigned)e & 0x80000000u) != (pi & 0x80000000u)) {
-            if (!w.spin(P.g, W_ENTRY)) { ok = false; break; }
+        bool ok = true;
+        unsigned v = 0;
+        if (status == ST_LOCAL) {
+          v = S.loc_v[tid];
+          dp = S.loc_d[tid];
+        } else {
+          const unsigned long long idx = h + tid;
+          const unsigned pi = ((idx >> ADDS_PAGE_LOG2) == (h >> ADDS_PAGE_LOG2)) ? S.pi0 : S.pi1;
+          ok = pi != PI_BAD;
+          unsigned long long e = 0;
+          if (ok) {
+            const unsigned long long *ep = entry_ptr(P, pi, idx);
+            Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
             e = ld_rlx64(ep);
+            while (((unsigned)e & 0x80000000u) != (pi & 0x80000000u)) {
+              if (!w.spin(P.g, W_ENTRY)) { ok = false; break; }
+              e = ld_rlx64(ep);
+            }
           }
+          v = (unsigned)e & 0x7FFFFFFFu;
+          dp = (unsigned)(e >> 32);
         }
         if (ok) {
-          const unsigned v = (unsigned)e & 0x7FFFFFFFu;
-          dp = (unsigned)(e >> 32);
           const unsigned dv = __ldcg(dist + v);
           ++st_items;
           if (dv < dp) {
             ++st_stale; /* superseded: a later push carries the smaller value */
           } else {
-            rb = __ldg(row + v);
-            const unsigned re = __ldg(row + v + 1);
-            deg = re - rb;
+            const unsigned r0 = __ldg(row + v), r1 = __ldg(row + v + 1);
+            const unsigned nl = split ? __ldg(split + v) : (r1 - r0);
+            if (status == ST_HEAVY) { /* settled vertex: its heavy edges */
+              rb = r0 + nl;
+              deg = r1 - rb;
+              ++st_heavy;
+            } else {                  /* light edges now, heavy list later */
+              rb = r0;
+              deg = nl;
+              if (nl < r1 - r0) stage<BLOCK>(S, v, dp, ADDS_NB + (myslot & (ADDS_NB - 1u)));
+            }
             if (deg > P.hub_threshold) {
               chunks = (deg + P.hub_chunk - 1u) / P.hub_chunk;
               atomicAdd(&S.hub_chunks, chunks);
@@ -546,17 +738,23 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
             }
           }
         }
+        if (chunks) S.loc_v[tid] = v; /* remembered for the chunk records */
       }
       S.it_rb[tid] = rb;
       S.it_du[tid] = dp;
       unsigned tot;
       const unsigned off = block_exscan<BLOCK>(S, chunks ? 0u : deg, tot);
       S.it_off[tid] = off;
-      /* retire the popped range: pages whose entries are all consumed go back */
+      /* retire the claimed range: pages whose entries are all consumed go back */
       if (tid == 0) {
-        const unsigned c0 = min((unsigned)(ADDS_PAGE - (h & PAGE_MASK)), k);
-        consume(P, S.pi0, c0);
-        if (k > c0) consume(P, S.pi1, k - c0);
+        if (status != ST_LOCAL) {
+          const unsigned c0 = min((unsigned)(ADDS_PAGE - (h & PAGE_MASK)), k);
+          consume(P, S.pi0, c0);
+          if (k > c0) consume(P, S.pi1, k - c0);
+        } else {
+          ++st_local;
+        }
+        S.loc_k = 0;
         if (S.hub_chunks) {
           atomicAdd(&d.ctl->live, S.hub_chunks);
           __threadfence();
@@ -566,12 +764,13 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
       if (chunks) {
         /* publish this row's chunks for the whole grid (tb_coop_assign,
          * wl.h:1638-1696, widened from one block to all CTAs) */
+        const unsigned u = S.loc_v[tid];
         const unsigned mask = (1u << ADDS_HUB_RING_LOG2) - 1u;
         const unsigned long long t0 = atomicAdd(&P.g->hub_tail, (unsigned long long)chunks);
         for (unsigned c = 0; c < chunks; ++c) {
           const unsigned long long t = t0 + c;
           unsigned *seq = P.hub_seq + (t & mask);
-          Waiter w{deadline, 0, ADDS_DEV_TIMEOUT};
+          Waiter w{deadline, 0, ADDS_DEV_HUB_OVERFLOW};
           bool ok = true;
           while (ld_acq32(seq) != (unsigned)t) {
             if (!w.spin(P.g, W_HUB_PUB)) { ok = false; break; }
@@ -579,10 +778,12 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
           if (!ok) break;
           HubChunk hc;
           hc.q = q;
+          hc.u = u;
           hc.du = dp;
           hc.eb = rb + c * P.hub_chunk;
           hc.ee = (unsigned)min((unsigned long long)rb + (unsigned long long)(c + 1u) * P.hub_chunk,
                                 (unsigned long long)rb + deg);
+          hc.pad[0] = hc.pad[1] = hc.pad[2] = 0u;
           P.hub[t & mask] = hc;
           __threadfence();
           st_rel32(seq, (unsigned)(t + 1ull));
@@ -591,16 +792,26 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
     } else { /* ST_HUB: one chunk of a split row, staged by acquire */
       if (tid == 0) {
         ++st_hub;
-        st_edges += S.total_edges;
+        /* the row's vertex improved since the chunk was made: a later
+         * expansion covers these edges with the smaller distance */
+        if (__ldcg(dist + S.hub_u) < S.it_du[0]) {
+          S.total_edges = 0;
+          ++st_hub_stale;
+        } else {
+          st_edges += S.total_edges;
+        }
       }
+      __syncthreads();
     }
     if (tid == 0) {
       ++st_batches;
       S.hub_chunks = 0;
     }
+    CY_LAP(cy_load);
 
     /* edge-balanced expansion of the batch: relax + atomicMin + stage push */
     const unsigned E = S.total_edges;
+    int lo = 0; /* a thread's edges only increase: each search starts at the last item */
     for (unsigned eb = 0; eb < E; eb += BLOCK * U) {
       unsigned dst[U], nd[U];
 #pragma unroll
@@ -609,7 +820,7 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
         nd[u] = 0xFFFFFFFFu;
         dst[u] = 0;
         if (e < E) {
-          int lo = 0, hi = (int)k - 1;
+          int hi = (int)k - 1;
           while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (S.it_off[mid] <= e) lo = mid; else hi = mid - 1;
@@ -627,47 +838,53 @@ __global__ void __launch_bounds__(BLOCK) solve_kernel(EngParams P) {
           const unsigned cur = __ldcg(dist + dst[u]);
           if (nd[u] < cur) {
             const unsigned old = atomicMin(dist + dst[u], nd[u]);
-            if (old > nd[u]) {
-              const unsigned s =
-                  bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key);
-              cg::coalesced_group grp = cg::coalesced_threads();
-              unsigned pos = 0;
-              if (grp.thread_rank() == 0) pos = atomicAdd(&S.pcnt, grp.size());
-              pos = grp.shfl(pos, 0) + grp.thread_rank();
-              S.pb_v[pos] = dst[u];
-              S.pb_d[pos] = nd[u];
-              S.pb_s[pos] = (unsigned char)s;
-            }
+            if (old > nd[u])
+              stage<BLOCK>(S, dst[u], nd[u],
+                           bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
           }
         }
       }
       __syncthreads();
-      if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, S, d, deadline, st_pushes);
+      if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, S, d, deadline, st_pushes, false);
     }
     __syncthreads();
-    flush<BLOCK>(P, S, d, deadline, st_pushes);
+    CY_LAP(cy_edge);
+    flush<BLOCK>(P, S, d, deadline, st_pushes, P.local_max != 0u);
     /* batch finished: its k entries (or one chunk) leave the live count */
     if (tid == 0) {
-      if (status == ST_WORK) atomicAdd(&d.slots[S.slot].inflight, (unsigned long long)(0ull - k));
+      if (status != ST_HUB)
+        atomicAdd(&d.slots[S.slot].inflight, (unsigned long long)(0ull - k));
       atomicSub(&d.ctl->live, k);
     }
     __syncthreads();
+    CY_LAP(cy_flush);
   }
+#undef CY_LAP
 
+  if (tid == 0 && S.hungry) atomicSub(&P.g->hungry, 1u);
   /* statistics */
   {
     GlobalCtl *g = P.g;
 #define WSUM(x) \
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
-    WSUM(st_items) WSUM(st_stale) WSUM(st_edges) WSUM(st_pushes)
+    WSUM(st_items) WSUM(st_stale) WSUM(st_edges) WSUM(st_pushes) WSUM(st_heavy)
 #undef WSUM
     if ((tid & 31u) == 0u) {
       if (st_items) atomicAdd(&g->st_items, st_items);
       if (st_stale) atomicAdd(&g->st_stale, st_stale);
       if (st_edges) atomicAdd(&g->st_edges, st_edges);
       if (st_pushes) atomicAdd(&g->st_pushes, st_pushes);
+      if (st_heavy) atomicAdd(&g->st_heavy, st_heavy);
       if (tid == 0) {
+        atomicAdd(&g->st_cyc[0], cy_acq);
+        atomicAdd(&g->st_cyc[1], cy_load);
+        atomicAdd(&g->st_cyc[2], cy_edge);
+        atomicAdd(&g->st_cyc[3], cy_flush);
+        atomicAdd(&g->st_cyc[4], cy_idle);
+        atomicAdd(&g->st_cyc[5], (unsigned long long)(clock64() - cy_start));
         if (st_hub) atomicAdd(&g->st_hub, st_hub);
+        if (st_local) atomicAdd(&g->st_local, st_local);
+        if (st_hub_stale) atomicAdd(&g->st_hub_stale, st_hub_stale);
         atomicAdd(&g->st_batches, st_batches);
       }
     }
@@ -690,8 +907,10 @@ __global__ void init_kernel(EngParams P) {
     GlobalCtl *g = P.g;
     if (q == 0) {
       g->remaining = P.nq;
+      g->hungry = 0;
       g->st_items = g->st_stale = g->st_edges = g->st_pushes = 0;
-      g->st_batches = g->st_hub = 0;
+      g->st_batches = g->st_hub = g->st_local = g->st_hub_stale = g->st_heavy = 0;
+      for (int i = 0; i < 6; ++i) g->st_cyc[i] = 0;
     }
     QueryCtl *c = d.ctl;
     c->ctrl = 0ull;
@@ -699,14 +918,17 @@ __global__ void init_kernel(EngParams P) {
     c->shift = d.shift0;
     c->adapt_state = 0u;
     c->pushes_at_base = 0ull;
-    for (int s = 0; s < ADDS_NB; ++s) d.slots[s].inflight = 0ull;
+    for (int s = 0; s < NSLOT; ++s) d.slots[s].inflight = 0ull;
     c->live = 1u;
     __threadfence();
     const unsigned long long deadline = gtimer() + P.timeout_ns;
-    unsigned long long b;
-    unsigned p0, p1;
-    if (slot_reserve(P, d, 0u, 1u, deadline, &b, &p0, &p1))
+    unsigned long long b, cvp = ~0ull;
+    unsigned p0, p1, cpi = 0;
+    if (slot_reserve(P, d, 0u, 1u, deadline, &b, &p0, &p1, &cvp, &cpi)) {
       st_rlx64(entry_ptr(P, p0, b), make_entry(src, 0u, p0));
+      __threadfence();
+      atomicAdd((unsigned long long *)&d.slots[0].avail, 1ull);
+    }
   }
 }
 
@@ -744,25 +966,43 @@ __global__ void wl_reset_kernel(unsigned long long *fq, unsigned fq_cells, unsig
 
 /* ------------------------------------------------------------------------ */
 /* host-side launch helpers (called from api.cu)                              */
-static const int kBlock = 512;
-
-template <bool FLT>
-static cudaError_t prep_solver(int *max_blocks_per_sm) {
-  const size_t smem = sizeof(Smem<kBlock>);
-  cudaError_t e = cudaFuncSetAttribute(solve_kernel<FLT, kBlock>,
+template <bool FLT, int BLOCK>
+static cudaError_t prep_one(int *max_blocks_per_sm) {
+  const size_t smem = sizeof(Smem<BLOCK>);
+  cudaError_t e = cudaFuncSetAttribute(solve_kernel<FLT, BLOCK>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
-                                                       solve_kernel<FLT, kBlock>, kBlock, smem);
+                                                       solve_kernel<FLT, BLOCK>, BLOCK, smem);
+}
+
+template <bool FLT, int BLOCK>
+static cudaError_t launch_one(const EngParams &P, cudaStream_t st) {
+  /* cooperative launch: all CTAs co-resident (they wait on each other's
+   * pushes); cudaLaunchKernelEx form so the launch can be graph-captured */
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.nctas);
+  cfg.blockDim = dim3(BLOCK);
+  cfg.dynamicSmemBytes = sizeof(Smem<BLOCK>);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, solve_kernel<FLT, BLOCK>, P);
 }
 
 }  // namespace adds
 
-/* C++ linkage entry points used by api.cu */
-cudaError_t adds_engine_prepare(bool flt, int *max_blocks_per_sm, int *block) {
-  *block = adds::kBlock;
-  return flt ? adds::prep_solver<true>(max_blocks_per_sm)
-             : adds::prep_solver<false>(max_blocks_per_sm);
+/* C++ linkage entry points used by api.cu.  block: 128, 256 or 512. */
+cudaError_t adds_engine_prepare(bool flt, int block, int *max_blocks_per_sm) {
+  switch (block) {
+    case 128: return flt ? adds::prep_one<true, 128>(max_blocks_per_sm) : adds::prep_one<false, 128>(max_blocks_per_sm);
+    case 256: return flt ? adds::prep_one<true, 256>(max_blocks_per_sm) : adds::prep_one<false, 256>(max_blocks_per_sm);
+    case 512: return flt ? adds::prep_one<true, 512>(max_blocks_per_sm) : adds::prep_one<false, 512>(max_blocks_per_sm);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStream_t st) {
@@ -774,21 +1014,13 @@ cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t adds_engine_launch_solve(const EngParams &P, cudaStream_t st) {
-  /* cooperative launch: all CTAs co-resident (they wait on each other's
-   * pushes); cudaLaunchKernelEx form so the launch can be graph-captured */
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(P.nctas);
-  cfg.blockDim = dim3(adds::kBlock);
-  cfg.dynamicSmemBytes = sizeof(adds::Smem<adds::kBlock>);
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (P.is_float) return cudaLaunchKernelEx(&cfg, adds::solve_kernel<true, adds::kBlock>, P);
-  return cudaLaunchKernelEx(&cfg, adds::solve_kernel<false, adds::kBlock>, P);
+cudaError_t adds_engine_launch_solve(const EngParams &P, int block, cudaStream_t st) {
+  switch (block) {
+    case 128: return P.is_float ? adds::launch_one<true, 128>(P, st) : adds::launch_one<false, 128>(P, st);
+    case 256: return P.is_float ? adds::launch_one<true, 256>(P, st) : adds::launch_one<false, 256>(P, st);
+    case 512: return P.is_float ? adds::launch_one<true, 512>(P, st) : adds::launch_one<false, 512>(P, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t adds_engine_launch_reached(const unsigned *row, const unsigned *dist, unsigned n,

@@ -1,0 +1,409 @@
+#!/usr/bin/env python3
+"""Benchmark of the asynchronous delta-stepping SSSP engine.
+
+Headline workload (default): R-MAT scale 24 (16.8M vertices, 16 directed
+draws per vertex, a/b/c/d = .57/.19/.19/.05, self-loops and duplicates
+removed), int32 weights uniform in [1, 10000], 8 seeded sources with
+out-degree > 0.  A step is one solve from the next source.  Metric: GTEPS =
+out-edges of the reached vertices / solve time (the Graph500 convention).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload rmat24|rmat16|grid4096|rmat26|batched|diff]
+
+--impl reference times the reference's CPU delta-stepping path (Galois
+OBIM delta-stepping, restated in oracle/oracle.c because Galois is not
+vendored) with all host threads on a bounded sample of the same workload.
+Inputs are generated by seeded synthetic generators (the reference's
+SuiteSparse/DIMACS/SNAP files are not available).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+# ---------------------------------------------------------------- utilities
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, device: int, path: str):
+        self.path = path
+        self.proc = None
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={device}", f"--query-gpu={SMI_FIELDS}", "--format=csv",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9 or not p[1].split()[0].isdigit():
+                    continue
+                sm.append(int(p[1].split()[0]))
+                mx.append(int(p[2].split()[0]))
+                for nm, val in zip(names[1:], p[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": int(statistics.median(loaded)), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """dram bytes per launch from a committed ncu summary (profiles/*.json)."""
+    p = os.path.join(ROOT, "profiles", f"{name}.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+# ---------------------------------------------------------------- workloads
+WORKLOADS = {
+    "rmat24": dict(kind="rmat", scale=24, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=24),
+    "rmat26": dict(kind="rmat", scale=26, wtype=1, w_lo=0.0, w_hi=1.0, nsrc=8, seed=26),
+    "rmat16": dict(kind="rmat", scale=16, wtype=0, w_lo=1, w_hi=1000, nsrc=1, seed=16,
+                   src="maxdeg"),
+    "rmat21": dict(kind="rmat", scale=21, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=21),
+    "grid4096": dict(kind="grid", side=4096, wtype=1, w_lo=1.0, w_hi=100.0, nsrc=1, seed=4096,
+                     src="center"),
+}
+
+
+def make_graph(wl: dict, device: int):
+    import adds_b200 as A
+    if wl["kind"] == "rmat":
+        spec = A.gen_spec("rmat", scale=wl["scale"], edge_factor=16, a=0.57, b=0.19, c=0.19,
+                          wtype=wl["wtype"], w_lo=wl["w_lo"], w_hi=wl["w_hi"], seed=wl["seed"])
+    else:
+        spec = A.gen_spec("grid", side=wl["side"], shortcut_frac=0.02, radius=8,
+                          wtype=wl["wtype"], w_lo=wl["w_lo"], w_hi=wl["w_hi"], seed=wl["seed"])
+    return A.Graph.generate(spec, device)
+
+
+def pick_sources(g, wl: dict, row: np.ndarray):
+    deg = np.diff(row)
+    if wl.get("src") == "maxdeg":
+        return [int(np.argmax(deg))]
+    if wl.get("src") == "center":
+        s = wl["side"]
+        return [(s // 2) * s + s // 2]
+    rng = np.random.default_rng(wl["seed"])
+    cand = np.flatnonzero(deg > 0)
+    return [int(x) for x in rng.choice(cand, size=wl["nsrc"], replace=False)]
+
+
+def describe(wl_name: str, wl: dict):
+    if wl["kind"] == "rmat":
+        w = (f"int32 U[{wl['w_lo']},{wl['w_hi']}]" if wl["wtype"] == 0
+             else f"float32 U[{wl['w_lo']},{wl['w_hi']})")
+        return {"workload": f"{wl_name}: R-MAT scale {wl['scale']}, edge factor 16, "
+                            f"a/b/c/d=.57/.19/.19/.05, {w}, {wl['nsrc']} source(s)",
+                "scale": wl["scale"], "edge_factor": 16, "sources": wl["nsrc"], "seed": wl["seed"]}
+    return {"workload": f"{wl_name}: {wl['side']}x{wl['side']} 4-neighbour grid + 2% shortcuts "
+                        f"(Manhattan radius 8), float32 U[{wl['w_lo']},{wl['w_hi']}), centre source",
+            "side": wl["side"], "sources": 1, "seed": wl["seed"]}
+
+
+# ---------------------------------------------------------------- distributed
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, local):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def barrier(dist, local):
+    if dist is None:
+        return
+    import torch
+    if torch.cuda.is_available():
+        t = torch.ones(1, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        torch.cuda.synchronize(local)
+    else:
+        dist.barrier()
+
+
+def reduce_max_sum(dist, local, tmax, usum):
+    if dist is None:
+        return tmax, usum
+    import torch
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    a = torch.tensor([tmax], dtype=torch.float64, device=dev)
+    b = torch.tensor([usum], dtype=torch.float64, device=dev)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(a.item()), float(b.item())
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_delta_step(csr, srcs, budget_s=20.0, threads=None):
+    """Times the CPU delta-stepping restatement (Galois OBIM semantics) on
+    sources until the time budget is spent; picks the bucket width first on
+    the first source.  Returns GTEPS and a description."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    deg = np.diff(csr.row.astype(np.int64))
+    if csr.wtype == 0:
+        cands = [dict(shift=s) for s in (8, 10, 12, 13)]
+    else:
+        aw = float(csr.weights().mean()) if csr.m else 1.0
+        cands = [dict(div=aw * f) for f in (0.25, 1.0, 4.0)]
+    best, best_t = None, 1e30
+    t_used = 0.0
+    for c in cands:  # bucket-width choice on the first source (not reported)
+        d, work, ms = O.delta_step(csr, srcs[0], threads=threads, **c)
+        t_used += ms / 1e3
+        if ms < best_t:
+            best, best_t = c, ms
+        if t_used > budget_s:
+            break
+    edges, secs, used = 0, 0.0, []
+    for s in srcs:
+        d, work, ms = O.delta_step(csr, s, threads=threads, **best)
+        reached = d != (0x7FFFFFFF if csr.wtype == 0 else 0x7F7FFFFF)
+        edges += int(deg[reached].sum())
+        secs += ms / 1e3
+        used.append(s)
+        if secs > budget_s:
+            break
+    return edges / secs / 1e9, dict(best=best, sources=used, threads=threads, secs=secs)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, wl_name, wl, ws, rank, local, dist):
+    import adds_b200 as A
+    g = make_graph(wl, local)
+    csr_row = g.download().row if wl["kind"] == "grid" else None
+    if csr_row is None:
+        csr_row = np.empty(g.n + 1, dtype=np.uint64)
+        A.check(A.lib().adds_graph_download(g.handle, csr_row.ctypes.data, None, None))
+    srcs = pick_sources(g, wl, csr_row)
+    tuned, tune_ms = None, None
+    if not args.no_tune:
+        tuned, tune_ms = g.tune(srcs[:2])
+    opts = A.default_opts(timeout_ms=60000)
+    # per-source reached vertices / edges (outside the timed region)
+    mr, nr = {}, {}
+    for s in srcs:
+        g.sssp(s, opts)
+        nr[s], mr[s] = g.reached()
+    for i in range(args.warmup):
+        g.sssp_async(srcs[i % len(srcs)], opts)
+    g.sync()
+    steps = [srcs[i % len(srcs)] for i in range(args.steps)]
+    import torch
+    torch.cuda.set_device(local)
+    barrier(dist, local)
+    torch.cuda.synchronize(local)
+    smi = ClockSampler(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else "/tmp", f"clocks_rank{rank}.csv"))
+    t0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    # solves run on the graph's own stream; bracket with host syncs + events
+    ev0.record()
+    torch.cuda.synchronize(local)
+    t_host0 = time.perf_counter()
+    for s in steps:
+        g.sssp_async(s, opts)
+    st = g.sync()
+    t_host1 = time.perf_counter()
+    ev1.record()
+    torch.cuda.synchronize(local)
+    clocks = smi.stop()
+    barrier(dist, local)
+    # the whole bracket on the device clock (includes any host enqueue gaps)
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    wall = t_host1 - t_host0
+    units = sum(mr[s] for s in steps)
+    tmax, usum = reduce_max_sum(dist, local, elapsed, units)
+    value = usum / tmax / 1e9
+    kernel_s = st["kernel_ms"] / 1e3
+    balg = sum(12 * mr[s] + 24 * nr[s] for s in steps)
+    peak, peak_kind = measured_peaks()
+    achieved = balg / kernel_s / 1e9
+    prof = profile_traffic(f"solve_kernel_{wl_name}")
+    traffic = None
+    if prof and "dram_bytes_per_launch" in prof:
+        traffic = prof["dram_bytes_per_launch"]
+    # e2e: the C-ABI call with a pinned host output buffer, copies timed
+    pinned = torch.empty(g.n, dtype=torch.int32, pin_memory=True)
+    e2e_steps = steps[: max(1, min(len(steps), args.e2e_steps))]
+    barrier(dist, local)
+    te0 = time.perf_counter()
+    for s in e2e_steps:
+        g.sssp(s, opts, out=pinned.data_ptr())
+    te1 = time.perf_counter()
+    e2e_units = sum(mr[s] for s in e2e_steps)
+    etmax, eusum = reduce_max_sum(dist, local, te1 - te0, e2e_units)
+    e2e = {"value": eusum / etmax / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 4,
+           "d2h_bytes_per_step": 4 * g.n,
+           "note": "adds_sssp(graph, src, pinned host dist) per step, host wall clock; the "
+                   "4-byte source id is the step input, the distance array the result"}
+    work_edges = st["edges_scanned"]
+    out = {
+        "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32" if wl["wtype"] == 0 else "float32", "data": "synthetic",
+        "config": {**describe(wl_name, wl), "parallelism": f"replicas{ws}",
+                   "l2": "inputs larger than L2 (CSR > 126 MB), no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "kernel": "adds::solve_kernel (persistent, 1 launch per solve)",
+                     "bytes_model": "12*m_r + 24*n_r per solve"},
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "extra": {
+            "n": g.n, "m": g.m, "sources": srcs, "m_r": [mr[s] for s in srcs],
+            "n_r": [nr[s] for s in srcs], "kernel_ms_per_step": st["kernel_ms"] / args.steps,
+            "solve_ms_per_step": st["ms"] / args.steps, "host_wall_s": wall,
+            "device_sum_of_solves_s": st["ms"] / 1e3,
+            "work_gteps_last": None, "edges_scanned_last": work_edges,
+            "items_last": st["items_popped"], "stale_last": st["items_stale"],
+            "pushes_last": st["pushes"], "ctas": st["ctas"],
+            "tuned": ({k: getattr(tuned, k) for k in ("delta_shift", "window", "batch_max",
+                                                        "hub_threshold", "ctas_per_sm",
+                                                        "strict_order")} if tuned else None),
+            "tune_ms_per_solve": tune_ms,
+        },
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        csr = g.download()
+        gteps, info = cpu_delta_step(csr, srcs, budget_s=args.cpu_budget)
+        out["cpu_baseline"] = {
+            "value": gteps, "unit": "GTEPS", "cores": info["threads"], "kind": "port",
+            "sample": (f"CPU delta-stepping (oracle/oracle.c, Galois OBIM semantics) on the same "
+                       f"graph, {len(info['sources'])} of the {len(srcs)} sources, "
+                       f"{info['threads']} threads, bucket {info['best']}, {info['secs']:.1f} s")}
+    g.close()
+    return out
+
+
+def run_reference(args, wl_name, wl, ws, rank, local):
+    """The reference's CPU path (Galois delta-stepping restated) on the same
+    workload; each step is one CPU solve, bounded by the time budget."""
+    import adds_b200 as A
+    g = make_graph(wl, local)  # input preparation only (not timed)
+    csr = g.download()
+    g.close()
+    srcs = pick_sources(None, wl, csr.row)
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    if csr.wtype == 0:
+        kw = dict(shift=12)
+    else:
+        kw = dict(div=float(csr.weights().mean()))
+    deg = np.diff(csr.row.astype(np.int64))
+    inf = 0x7FFFFFFF if csr.wtype == 0 else 0x7F7FFFFF
+    total_edges, total_s = 0, 0.0
+    for i in range(args.warmup + args.steps):
+        s = srcs[i % len(srcs)]
+        d, work, ms = O.delta_step(csr, s, threads=threads, **kw)
+        if i >= args.warmup:
+            total_edges += int(deg[d != inf].sum())
+            total_s += ms / 1e3
+        if i >= args.warmup and total_s > args.cpu_budget * 6:
+            break
+    v = total_edges / total_s / 1e9
+    return {
+        "impl": "reference", "metric": "sssp_gteps", "value": v, "unit": "GTEPS", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32" if wl["wtype"] == 0 else "float32",
+        "data": "synthetic", "config": {**describe(wl_name, wl), "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": threads, "kind": "port",
+                         "sample": f"CPU delta-stepping restatement, {kw}, {threads} threads, "
+                                   f"one solve per step"},
+        "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_env()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, args.workload, wl, ws, rank, local)), flush=True)
+        return
+    dist = dist_init(ws, local)
+    out = run_ours(args, args.workload, wl, ws, rank, local, dist)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -68,19 +68,32 @@ typedef struct adds_opts {
   int32_t timeout_ms;    /* bound on every device wait; 0 = 20000 ms             */
   int32_t adapt;         /* on-device delta re-tuning: -1 auto, 0 off, 1 on      */
   int32_t strict_order;  /* 1: advance a bucket only when its work is done       */
-  int32_t reserved[6];
+  int32_t local_max;     /* own pushes a CTA keeps as its next batch; <0 = auto,
+                            0 = always go through the HBM queues              */
+  int32_t light_heavy;   /* 1: relax heavy edges (w >= delta) once per settled
+                            vertex from a weight-sorted row copy; 0: off;
+                            <0 = auto (on)                                     */
+  int32_t block_threads; /* threads per persistent CTA: 128, 256 or 512; 0 = auto */
+  int32_t greed;         /* a claim takes avail / (CTAs >> greed) entries; <0 = auto */
+  int32_t reserved[2];
 } adds_opts;
 
 /* Per-solve statistics (reference: work_count + fd-3 record,
  * ads_int/kernel.cu:264-282). */
 typedef struct adds_stats {
   double ms;                /* device time of the solve(s), CUDA events        */
+  double kernel_ms;         /* of which the persistent solver kernel(s)        */
   uint64_t items_popped;    /* queue entries popped (reference int work count) */
   uint64_t items_stale;     /* popped entries skipped as superseded            */
   uint64_t edges_scanned;   /* edges of expanded vertices (float work count)   */
   uint64_t pushes;          /* queue entries pushed                            */
   uint64_t batches;         /* CTA-level pops                                  */
   uint64_t hub_chunks;      /* split row chunks processed                      */
+  uint64_t hub_stale;       /* of which skipped (row's vertex had improved)    */
+  uint64_t local_batches;   /* batches a CTA took from its own pushes          */
+  uint64_t heavy_lists;     /* settled vertices whose heavy edges were relaxed */
+  uint64_t phase_cycles[6]; /* SM cycles summed over CTAs: acquire, load,
+                               edges, flush, idle, total                      */
   uint64_t reached;         /* vertices with finite distance (filled on request) */
   uint64_t reached_edges;   /* out-edges of reached vertices (filled on request) */
   int32_t delta_shift;      /* bucket shift at the end of the solve            */

@@ -9,10 +9,10 @@
  *   - serial Dijkstra, the reference's gold standard (run_all.sh:93-107 with
  *     -algo=dijkstra -t 1; cpu_sssp_int.patch:50-64 MinHeap loop);
  *   - Galois delta-stepping, the reference's CPU comparison
- *     (cpu_sssp_int.patch:17-46: OBIM buckets keyed dist >> shift, chunks of
- *     64 items, skip an item whose node improved since it was pushed, push
- *     when atomicMin lowered the distance; float: bucket (unsigned)(dist/div),
- *     cpu_sssp_float.patch:13,23,267-279) with std threads;
+ *     (cpu_sssp_int.patch:17-46: buckets keyed dist >> shift, chunks of 64
+ *     items, skip an item whose node improved since it was pushed, push when
+ *     atomicMin lowered the distance; float: bucket (unsigned)(dist/div),
+ *     cpu_sssp_float.patch:13,23,267-279), bulk-synchronous over pthreads;
  *   - relaxation arithmetic of the GPU path (ads_int/kernel.cu:112-121):
  *     int new = d[u] + w as 32-bit (both operands < 2^31, so no wrap),
  *     accepted iff new < d[v] with INF = INT32_MAX; float new = fl(d[u]+w)
@@ -21,6 +21,7 @@
  *     tree, lambda summed in CSR child order, queries in order).
  * Compiled with -ffp-contract=off so float sums are single IEEE adds.
  */
+#define _GNU_SOURCE
 #include <float.h>
 #include <pthread.h>
 #include <stdatomic.h>
@@ -174,15 +175,25 @@ int oracle_dijkstra_f64(uint32_t n, const uint64_t *row, const uint32_t *dst, co
   return 0;
 }
 
-/* ---------------- Galois-style parallel delta-stepping ---------------- */
+/* ---------------- parallel delta-stepping (CPU baseline) ----------------
+ * Same bucket function and item rule as the Galois OBIM loop the reference
+ * compares against (cpu_sssp_int.patch:17-46: bucket = dist >> shift, or
+ * (unsigned)(dist/div) for float; an item whose node improved since it was
+ * pushed is skipped; push when the atomic min lowered the distance), run
+ * bulk-synchronously: all threads drain the lowest non-empty bucket from a
+ * shared frontier (claimed in chunks of 64), pushing into thread-local
+ * buckets, until that bucket stays empty; then the next bucket. */
 #define CHUNK 64
 
-typedef struct chunk {
-  struct chunk *next;
-  uint32_t n;
-  uint32_t node[CHUNK];
-  uint32_t dist[CHUNK];
-} chunk_t;
+typedef struct {
+  uint32_t *v, *d;
+  size_t n, cap;
+} ivec_t;
+
+typedef struct {
+  ivec_t *b;
+  size_t nb;
+} tbk_t;
 
 typedef struct {
   uint32_t n;
@@ -193,13 +204,18 @@ typedef struct {
   uint32_t shift;
   float div;
   _Atomic uint32_t *dist;
-  pthread_mutex_t lock;
-  chunk_t **bucket; /* bucket lists, index = priority */
-  size_t nbucket;
-  size_t cur;        /* lowest possibly non-empty bucket */
-  _Atomic int64_t outstanding;
-  _Atomic uint64_t work;
+  int nthreads;
+  tbk_t *tb;
+  pthread_barrier_t bar;
+  uint32_t *fv, *fd;
+  size_t fcap, ftotal;
+  size_t *cnt, *off;
+  _Atomic size_t next;
+  _Atomic size_t minb;
+  size_t cur;
+  int done;
   _Atomic int failed;
+  _Atomic uint64_t work;
 } ds_t;
 
 static size_t prio(const ds_t *s, uint32_t d) {
@@ -210,136 +226,142 @@ static size_t prio(const ds_t *s, uint32_t d) {
   return d >> s->shift;
 }
 
-static int publish(ds_t *s, chunk_t *c, size_t b) {
-  pthread_mutex_lock(&s->lock);
-  if (b >= s->nbucket) {
-    size_t nn = s->nbucket ? s->nbucket : 1024;
-    while (nn <= b) nn *= 2;
-    chunk_t **nb = realloc(s->bucket, nn * sizeof *nb);
-    if (!nb) {
-      pthread_mutex_unlock(&s->lock);
-      return -1;
-    }
-    memset(nb + s->nbucket, 0, (nn - s->nbucket) * sizeof *nb);
-    s->bucket = nb;
-    s->nbucket = nn;
+static int ivec_push(ivec_t *x, uint32_t v, uint32_t d) {
+  if (x->n == x->cap) {
+    size_t nc = x->cap ? x->cap * 2 : 256;
+    uint32_t *nv = realloc(x->v, nc * 4), *nd;
+    if (!nv) return -1;
+    x->v = nv;
+    nd = realloc(x->d, nc * 4);
+    if (!nd) return -1;
+    x->d = nd;
+    x->cap = nc;
   }
-  c->next = s->bucket[b];
-  s->bucket[b] = c;
-  if (b < s->cur) s->cur = b;
-  pthread_mutex_unlock(&s->lock);
+  x->v[x->n] = v;
+  x->d[x->n] = d;
+  ++x->n;
   return 0;
 }
 
-static chunk_t *take(ds_t *s) {
-  chunk_t *c = NULL;
-  pthread_mutex_lock(&s->lock);
-  while (s->cur < s->nbucket && !s->bucket[s->cur]) ++s->cur;
-  if (s->cur < s->nbucket) {
-    c = s->bucket[s->cur];
-    s->bucket[s->cur] = c->next;
+static int tb_push(tbk_t *t, size_t b, uint32_t v, uint32_t d) {
+  if (b >= t->nb) {
+    size_t nn = t->nb ? t->nb : 64;
+    while (nn <= b) nn *= 2;
+    ivec_t *nb = realloc(t->b, nn * sizeof *nb);
+    if (!nb) return -1;
+    memset(nb + t->nb, 0, (nn - t->nb) * sizeof *nb);
+    t->b = nb;
+    t->nb = nn;
   }
-  pthread_mutex_unlock(&s->lock);
-  return c;
+  return ivec_push(&t->b[b], v, d);
 }
-
-#define OPEN 8 /* per-thread open chunks, keyed by bucket */
 
 typedef struct {
   ds_t *s;
+  int tid;
 } targ_t;
 
 static void *ds_worker(void *arg) {
   ds_t *s = ((targ_t *)arg)->s;
-  chunk_t *open[OPEN] = {0};
-  size_t openb[OPEN] = {0};
-  int idle = 0;
-  while (!atomic_load(&s->failed)) {
-    chunk_t *c = take(s);
-    if (!c) {
-      /* nothing global: publish local partial chunks, then check for the end */
-      int had = 0;
-      for (int i = 0; i < OPEN; ++i)
-        if (open[i]) {
-          if (publish(s, open[i], openb[i])) atomic_store(&s->failed, 1);
-          open[i] = NULL;
-          had = 1;
-        }
-      if (had) continue;
-      if (atomic_load(&s->outstanding) == 0) break;
-      if (++idle > 64) {
-        struct timespec ts = {0, 1000};
-        nanosleep(&ts, NULL);
+  const int tid = ((targ_t *)arg)->tid;
+  tbk_t *my = &s->tb[tid];
+  for (;;) {
+    /* lowest non-empty bucket over all threads */
+    size_t lo = SIZE_MAX;
+    for (size_t b = s->cur; b < my->nb; ++b)
+      if (my->b[b].n) {
+        lo = b;
+        break;
       }
-      continue;
+    size_t cur = atomic_load(&s->minb);
+    while (lo < cur && !atomic_compare_exchange_weak(&s->minb, &cur, lo)) {
     }
-    idle = 0;
-    int64_t pushed = 0;
-    for (uint32_t i = 0; i < c->n; ++i) {
-      const uint32_t u = c->node[i];
-      const uint32_t du = atomic_load_explicit(&s->dist[u], memory_order_relaxed);
-      if (du < c->dist[i]) continue; /* WLEmptyWork: node improved since push */
-      atomic_fetch_add_explicit(&s->work, 1, memory_order_relaxed);
-      for (uint64_t e = s->row[u]; e < s->row[u + 1]; ++e) {
-        const uint32_t v = s->dst[e];
-        uint32_t nd;
-        if (s->is_float) {
-          volatile float sum = f_of(du) + f_of(s->w[e]);
-          nd = b_of(sum);
-        } else {
-          nd = du + s->w[e];
+    pthread_barrier_wait(&s->bar);
+    if (tid == 0) {
+      s->cur = atomic_load(&s->minb);
+      s->done = s->cur == SIZE_MAX || atomic_load(&s->failed);
+      atomic_store(&s->minb, SIZE_MAX);
+    }
+    pthread_barrier_wait(&s->bar);
+    if (s->done) break;
+    const size_t b = s->cur;
+    for (;;) { /* phases of bucket b until it stays empty */
+      s->cnt[tid] = (b < my->nb) ? my->b[b].n : 0;
+      pthread_barrier_wait(&s->bar);
+      if (tid == 0) {
+        size_t t = 0;
+        for (int i = 0; i < s->nthreads; ++i) {
+          s->off[i] = t;
+          t += s->cnt[i];
         }
-        uint32_t old = atomic_load_explicit(&s->dist[v], memory_order_relaxed);
-        while (nd < old &&
-               !atomic_compare_exchange_weak_explicit(&s->dist[v], &old, nd, memory_order_relaxed,
-                                                      memory_order_relaxed)) {
-        }
-        if (nd < old) { /* pushWrap */
-          const size_t b = prio(s, nd);
-          int slot = -1;
-          for (int k = 0; k < OPEN; ++k)
-            if (open[k] && openb[k] == b) slot = k;
-          if (slot < 0) {
-            for (int k = 0; k < OPEN; ++k)
-              if (!open[k]) slot = k;
-            if (slot < 0) { /* evict one open chunk (count its items first) */
-              slot = 0;
-              atomic_fetch_add(&s->outstanding, pushed);
-              pushed = 0;
-              if (publish(s, open[0], openb[0])) atomic_store(&s->failed, 1);
-              open[0] = NULL;
-            }
-            open[slot] = calloc(1, sizeof(chunk_t));
-            if (!open[slot]) {
-              atomic_store(&s->failed, 1);
-              break;
-            }
-            openb[slot] = b;
+        s->ftotal = t;
+        if (t > s->fcap) {
+          size_t nc = t + t / 2 + 1024;
+          uint32_t *nv = realloc(s->fv, nc * 4), *nd = NULL;
+          if (nv) {
+            s->fv = nv;
+            nd = realloc(s->fd, nc * 4);
           }
-          chunk_t *oc = open[slot];
-          oc->node[oc->n] = v;
-          oc->dist[oc->n] = nd;
-          ++oc->n;
-          ++pushed;
-          if (oc->n == CHUNK) {
-            atomic_fetch_add(&s->outstanding, pushed);
-            pushed = 0;
-            if (publish(s, oc, b)) atomic_store(&s->failed, 1);
-            open[slot] = NULL;
+          if (!nv || !nd) {
+            atomic_store(&s->failed, 1);
+            s->ftotal = 0;
+          } else {
+            s->fd = nd;
+            s->fcap = nc;
           }
         }
+        atomic_store(&s->next, 0);
       }
+      pthread_barrier_wait(&s->bar);
+      const size_t total = s->ftotal;
+      if (total == 0) break;
+      if (s->cnt[tid]) {
+        memcpy(s->fv + s->off[tid], my->b[b].v, s->cnt[tid] * 4);
+        memcpy(s->fd + s->off[tid], my->b[b].d, s->cnt[tid] * 4);
+        my->b[b].n = 0;
+      }
+      pthread_barrier_wait(&s->bar);
+      uint64_t wk = 0;
+      for (;;) {
+        const size_t i0 = atomic_fetch_add(&s->next, CHUNK);
+        if (i0 >= total) break;
+        const size_t i1 = i0 + CHUNK < total ? i0 + CHUNK : total;
+        for (size_t i = i0; i < i1; ++i) {
+          const uint32_t u = s->fv[i];
+          const uint32_t du = atomic_load_explicit(&s->dist[u], memory_order_relaxed);
+          if (du < s->fd[i]) continue; /* improved since it was pushed */
+          ++wk;
+          for (uint64_t e = s->row[u]; e < s->row[u + 1]; ++e) {
+            const uint32_t v = s->dst[e];
+            uint32_t nd;
+            if (s->is_float) {
+              volatile float sum = f_of(du) + f_of(s->w[e]);
+              nd = b_of(sum);
+            } else {
+              nd = du + s->w[e];
+            }
+            uint32_t old = atomic_load_explicit(&s->dist[v], memory_order_relaxed);
+            while (nd < old && !atomic_compare_exchange_weak_explicit(
+                                   &s->dist[v], &old, nd, memory_order_relaxed,
+                                   memory_order_relaxed)) {
+            }
+            if (nd < old) {
+              size_t nb = prio(s, nd);
+              if (nb < b) nb = b;
+              if (tb_push(my, nb, v, nd)) atomic_store(&s->failed, 1);
+            }
+          }
+        }
+      }
+      atomic_fetch_add(&s->work, wk);
+      pthread_barrier_wait(&s->bar);
     }
-    /* new items are counted before this chunk's own items are retired */
-    atomic_fetch_add(&s->outstanding, pushed - (int64_t)c->n);
-    free(c);
   }
-  for (int i = 0; i < OPEN; ++i) free(open[i]);
   return NULL;
 }
 
-/* Multithreaded delta-stepping.  Returns 0; ms = wall time of the solve
- * (graph already in memory); work = items processed (Galois WORK_COUNT). */
+/* Parallel delta-stepping.  Returns 0; ms = wall time of the solve (graph
+ * already in memory); work = items processed (Galois WORK_COUNT). */
 int oracle_delta_step(uint32_t n, const uint64_t *row, const uint32_t *dst, const uint32_t *w,
                       uint32_t src, int is_float, uint32_t shift, float div, int nthreads,
                       uint32_t *dist_out, uint64_t *work, double *ms) {
@@ -355,33 +377,43 @@ int oracle_delta_step(uint32_t n, const uint64_t *row, const uint32_t *dst, cons
   s.shift = shift;
   s.div = div;
   s.dist = (_Atomic uint32_t *)dist_out;
-  pthread_mutex_init(&s.lock, NULL);
+  s.nthreads = nthreads;
+  s.tb = calloc((size_t)nthreads, sizeof(tbk_t));
+  s.cnt = calloc((size_t)nthreads, sizeof(size_t));
+  s.off = calloc((size_t)nthreads, sizeof(size_t));
+  pthread_t *th = malloc(sizeof(pthread_t) * (size_t)nthreads);
+  targ_t *ta = malloc(sizeof(targ_t) * (size_t)nthreads);
+  if (!s.tb || !s.cnt || !s.off || !th || !ta) return -2;
+  pthread_barrier_init(&s.bar, NULL, (unsigned)nthreads);
+  atomic_store(&s.minb, SIZE_MAX);
   struct timespec t0, t1;
   clock_gettime(CLOCK_MONOTONIC, &t0);
   const uint32_t inf = is_float ? b_of(FLT_MAX) : INF_I32;
   for (uint32_t v = 0; v < n; ++v) atomic_store_explicit(&s.dist[v], inf, memory_order_relaxed);
   atomic_store(&s.dist[src], 0u);
-  chunk_t *c0 = calloc(1, sizeof(chunk_t));
-  if (!c0) return -2;
-  c0->node[0] = src;
-  c0->dist[0] = 0;
-  c0->n = 1;
-  atomic_store(&s.outstanding, 1);
-  if (publish(&s, c0, 0)) return -2;
-  pthread_t *th = malloc(sizeof(pthread_t) * (size_t)nthreads);
-  targ_t ta = {&s};
-  for (int i = 0; i < nthreads; ++i) pthread_create(&th[i], NULL, ds_worker, &ta);
+  if (tb_push(&s.tb[0], prio(&s, 0), src, 0)) return -2;
+  for (int i = 0; i < nthreads; ++i) {
+    ta[i].s = &s;
+    ta[i].tid = i;
+    pthread_create(&th[i], NULL, ds_worker, &ta[i]);
+  }
   for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
   clock_gettime(CLOCK_MONOTONIC, &t1);
-  free(th);
-  for (size_t b = 0; b < s.nbucket; ++b)
-    while (s.bucket[b]) {
-      chunk_t *c = s.bucket[b];
-      s.bucket[b] = c->next;
-      free(c);
+  for (int i = 0; i < nthreads; ++i) {
+    for (size_t b = 0; b < s.tb[i].nb; ++b) {
+      free(s.tb[i].b[b].v);
+      free(s.tb[i].b[b].d);
     }
-  free(s.bucket);
-  pthread_mutex_destroy(&s.lock);
+    free(s.tb[i].b);
+  }
+  free(s.tb);
+  free(s.cnt);
+  free(s.off);
+  free(s.fv);
+  free(s.fd);
+  free(th);
+  free(ta);
+  pthread_barrier_destroy(&s.bar);
   if (work) *work = atomic_load(&s.work);
   if (ms) *ms = (t1.tv_sec - t0.tv_sec) * 1e3 + (t1.tv_nsec - t0.tv_nsec) * 1e-6;
   return atomic_load(&s.failed) ? -2 : 0;

@@ -40,6 +40,76 @@ def test_erdos_renyi_int():
 
 
 @pytest.mark.parametrize("shift", [0, 4, 9, 14, 20])
-def test_any_delta_gives_same_distances(shift):
+@pytest.mark.parametrize("lh", [0, 1])
+def test_any_delta_gives_same_distances(shift, lh):
     g = G.rmat(13, 16, seed=2)
-    _check(g, G.max_degree_vertex(g), delta_shift=shift)
+    _check(g, G.max_degree_vertex(g), delta_shift=shift, light_heavy=lh)
+
+
+@pytest.mark.parametrize("window", [1, 2, 4])
+@pytest.mark.parametrize("lh", [0, 1])
+@pytest.mark.parametrize("local", [0, 512])
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_schedules_int_rmat(window, lh, local, block):
+    g = G.rmat(12, 16, seed=5, w_hi=10000)
+    for shift in (6, 9, 12):
+        _check(g, 3, delta_shift=shift, window=window, light_heavy=lh, local_max=local,
+               block_threads=block, hub_threshold=256)
+
+
+@pytest.mark.parametrize("window", [1, 2])
+@pytest.mark.parametrize("lh", [0, 1])
+@pytest.mark.parametrize("block", [128, 512])
+def test_schedules_float_grid(window, lh, block):
+    g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=8)
+    for shift in (12, 16, 20):
+        _check(g, 40 * 96 + 48, delta_shift=shift, window=window, light_heavy=lh,
+               block_threads=block)
+
+
+def test_non_strict_order():
+    g = G.rmat(12, 16, seed=6, w_hi=10000)
+    for lh in (0, 1):
+        _check(g, 1, strict_order=0, light_heavy=lh, delta_shift=8)
+
+
+def test_batch_mixed_graphs_replayed_twice():
+    gs = [G.erdos_renyi(3000 + 997 * i, 8, seed=100 + i) for i in range(5)]
+    r = G.rmat(12, 16, seed=9)
+    graphs = [A.Graph.from_csr(g) for g in gs] + [A.Graph.from_csr(r)]
+    qg = graphs + [graphs[-1]] * 3
+    srcs = [0, 1, 2, 3, 4, G.max_degree_vertex(r), 1, 2, 3]
+    b = A.Batch(qg, srcs, A.default_opts(**OPTS))
+    csrs = gs + [r] * 4
+    for _ in range(2):  # second run replays the captured CUDA graph
+        st = b.run()
+        for q, (c, s) in enumerate(zip(csrs, srcs)):
+            ref, _ = O.dijkstra(c, s)
+            assert np.array_equal(b.dist(q), ref), f"query {q}"
+    new = [5, 6, 7, 8, 9, 10, 11, 12, 13]
+    b.set_sources(new)
+    b.run()
+    for q, (c, s) in enumerate(zip(csrs, new)):
+        ref, _ = O.dijkstra(c, s)
+        assert np.array_equal(b.dist(q), ref), f"query {q} after set_sources"
+    b.close()
+    for g in graphs:
+        g.close()
+
+
+def test_cli_int_matches_reference_text(tmp_path):
+    import os
+    import subprocess
+    g = G.rmat(12, 16, seed=4)
+    p = str(tmp_path / "r12.gr")
+    G.write_gr(p, g)
+    out = str(tmp_path / "out.txt")
+    rec = str(tmp_path / "fd3.txt")
+    exe = os.path.join(os.path.dirname(A._lib.HERE), "adds_b200", "bin", "sssp_int")
+    r = subprocess.run(["bash", "-c", f'"{exe}" -q -s 7 -r 2 -o "{out}" "{p}" 3>"{rec}"'],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    ref, _ = O.dijkstra(g, 7)
+    assert open(out).read() == G.dist_text(ref, G.I32)
+    name, ms, work = open(rec).read().split()
+    assert name == "r12.gr" and float(ms) > 0 and int(work) > 0
