@@ -155,6 +155,8 @@ SIGNATURES = [
     ("adds_tune", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Opts),
                             C.POINTER(C.c_double)]),
     ("adds_write_dist_text", C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_int]),
+    ("adds_sssp_noalloc", C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_uint32, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

@@ -60,6 +60,9 @@ static int cuda_fail(cudaError_t e, const char *what) {
     if (_e != cudaSuccess) return cuda_fail(_e, #x); \
   } while (0)
 
+/* diagnostics text for adds_last_cuda_error (used by noalloc.cu too) */
+void adds_set_last_error(const char *msg) { snprintf(g_last_err, sizeof g_last_err, "%s", msg); }
+
 extern "C" int adds_abi_version(void) { return ADDS_ABI_VERSION; }
 extern "C" const char *adds_last_cuda_error(void) { return g_last_err; }
 

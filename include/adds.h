@@ -214,6 +214,34 @@ int adds_sssp_backward(adds_graph *g, uint32_t ns, const uint32_t *srcs,
                        const float *dist, const float *grad_dist, float *grad_w,
                        const adds_opts *opts);
 
+/* ---- solve without allocating -------------------------------------------- */
+/* No counterpart in the reference.  For callers that may not let a library
+ * allocate device memory: a framework that owns all device memory through
+ * its own allocator or a fixed arena (a foreign cudaMalloc takes memory
+ * outside its budget; cudaFree synchronises the device), or a service loop
+ * that cannot afford those implicit synchronisations.  Nothing is allocated:
+ * the caller passes device arrays it owns, and the engine's working memory
+ * is one fixed device array of ADDS_NOALLOC_SCRATCH_BYTES inside this
+ * library, held on every GPU that loads the library until the process
+ * exits.
+ *   row_start: n+1 u32 row offsets; edges: 2*m u32 words, {dst, weight bits}
+ *   per edge in CSR order; dist: n words, overwritten (same INF values as
+ *   adds_sssp); all three on the current device.  stream: cudaStream_t or
+ *   NULL.  Returns after the solve has finished on that stream.
+ * Graphs above ADDS_NOALLOC_MAX_N vertices or ADDS_NOALLOC_MAX_M edges are
+ * rejected (ADDS_ERR_UNSUPPORTED); a graph within the limits whose queues
+ * outgrow the fixed pool reports ADDS_ERR_WL_OVERFLOW.  The first call on a
+ * device looks up the array's device address and prepares the kernels for
+ * that device; make that first call before any stream capture.  All calls
+ * share the array (each clears what it needs first): calls that overlap on
+ * the GPU race, so issue them one after another. */
+#define ADDS_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define ADDS_NOALLOC_MAX_N (1u << 20)
+#define ADDS_NOALLOC_MAX_M (1u << 24)
+int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_start,
+                      const uint32_t *edges, adds_wtype wt, uint32_t src,
+                      uint32_t *dist, void *stream);
+
 /* ---- autotuner ---------------------------------------------------------- */
 /* Times candidate (delta, window, CTAs/SM, batch, hub threshold) settings on
  * the sample sources and stores the fastest in the graph (used whenever a
