@@ -201,6 +201,20 @@ class Batch:
         check(lib().adds_batch_dist(self._h, q, _ptr(out)), "adds_batch_dist")
         return out
 
+    def layout(self):
+        """(offsets of each query in the flat distance array, total words)"""
+        off = np.empty(self.nq, dtype=np.uint64)
+        tot = C.c_uint64()
+        check(lib().adds_batch_dist_all(self._h, None, off.ctypes.data, C.byref(tot)),
+              "adds_batch_dist_all")
+        return off, tot.value
+
+    def dist_all(self, out) -> None:
+        """Copies every query's distances (flat, see layout()) to out."""
+        tot = C.c_uint64()
+        check(lib().adds_batch_dist_all(self._h, _ptr(out), None, C.byref(tot)),
+              "adds_batch_dist_all")
+
     def dist_ptr(self, q: int) -> int:
         p = C.c_void_p()
         check(lib().adds_batch_dist_ptr(self._h, q, C.byref(p)), "adds_batch_dist_ptr")

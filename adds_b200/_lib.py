@@ -73,6 +73,8 @@ class Stats(C.Structure):
         ("local_batches", C.c_uint64),
         ("heavy_lists", C.c_uint64),
         ("phase_cycles", C.c_uint64 * 6),
+        ("mid_flush_cycles", C.c_uint64),
+        ("mid_flushes", C.c_uint64),
         ("reached", C.c_uint64),
         ("reached_edges", C.c_uint64),
         ("delta_shift", C.c_int32),
@@ -147,6 +149,7 @@ SIGNATURES = [
     ("adds_batch_sync", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("adds_batch_dist", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     ("adds_batch_dist_ptr", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("adds_batch_dist_all", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
     ("adds_batch_set_sources", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
     ("adds_batch_free", None, [C.c_void_p]),
     ("adds_batch_backward", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),

@@ -113,7 +113,7 @@ struct __align__(128) GlobalCtl {
   unsigned long long st_heavy;    /* heavy-edge lists expanded                   */
   unsigned long long st_cyc[6];   /* SM cycles: acquire, load, edges, flush,
                                      idle, total (summed over CTAs)            */
-  unsigned long long st_pad[1];
+  unsigned long long st_pad[2];   /* diagnostics: mid-batch flush cycles, count */
 };
 
 /* Kernel parameters (passed by value). */

@@ -344,6 +344,8 @@ static void fill_stats(const Engine &E, const EngParams &P, adds_stats *s) {
   s->local_batches = g.st_local;
   s->heavy_lists = g.st_heavy;
   for (int i = 0; i < 6; ++i) s->phase_cycles[i] = g.st_cyc[i];
+  s->mid_flush_cycles = g.st_pad[0];
+  s->mid_flushes = g.st_pad[1];
   s->ctas = (int32_t)P.nctas;
 }
 
@@ -361,6 +363,11 @@ struct adds_graph {
   unsigned *split = nullptr;   /* light-edge count per row for split_thr      */
   unsigned split_thr = 0;
   bool sorted_valid = false, split_valid = false;
+  unsigned long long wversion = 0; /* bumped by adds_graph_set_weights */
+  unsigned *aux = nullptr;        /* 64 B: validation flag + weight sample sum */
+  uint32_t *sort_buf = nullptr;   /* 4*m words: keys/values in and out          */
+  void *sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
   cudaStream_t stream = nullptr;
   uint32_t max_deg = 0;
   double avg_deg = 0, avg_w = 0;
@@ -501,6 +508,9 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->dist) cudaFree(g->dist);
   if (g->sedges) cudaFree(g->sedges);
   if (g->split) cudaFree(g->split);
+  if (g->aux) cudaFree(g->aux);
+  if (g->sort_buf) cudaFree(g->sort_buf);
+  if (g->sort_tmp) cudaFree(g->sort_tmp);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   for (int i = 0; i < adds_graph::kRing; ++i)
@@ -717,28 +727,23 @@ extern "C" int adds_graph_set_weights(adds_graph *g, const void *w) {
     CK(cudaMemcpyAsync(tmp, w, g->m * 4, cudaMemcpyHostToDevice, g->stream));
     src = tmp;
   }
-  unsigned *bad = nullptr;
-  CK(cudaMalloc(&bad, 4));
-  CK(cudaMemsetAsync(bad, 0, 4, g->stream));
-  k_set_weights<<<592, 256, 0, g->stream>>>(g->edges, src, g->m, g->wt == ADDS_F32, bad);
-  unsigned hb = 0;
-  CK(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, g->stream));
+  if (!g->aux) CK(cudaMalloc(&g->aux, 64));
+  CK(cudaMemsetAsync(g->aux, 0, 64, g->stream));
+  k_set_weights<<<592, 256, 0, g->stream>>>(g->edges, src, g->m, g->wt == ADDS_F32, g->aux);
+  /* the weight sample feeds the automatic delta */
+  const unsigned ns = (unsigned)std::min<uint64_t>(g->m, 1u << 16);
+  k_sample_w<<<64, 256, 0, g->stream>>>(g->edges, g->m, g->wt == ADDS_F32, ns,
+                                         (double *)(g->aux + 2));
+  unsigned h[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(h, g->aux, 16, cudaMemcpyDeviceToHost, g->stream));
   CK(cudaStreamSynchronize(g->stream));
   if (tmp) cudaFree(tmp);
-  cudaFree(bad);
-  if (hb) return ADDS_ERR_INVALID;
-  g->sorted_valid = g->split_valid = false; /* the weight order changed */
-  /* the weight sample feeds the automatic delta */
-  double sw = 0;
-  double *d_sw = nullptr;
-  CK(cudaMalloc(&d_sw, 8));
-  CK(cudaMemsetAsync(d_sw, 0, 8, g->stream));
-  const unsigned ns = (unsigned)std::min<uint64_t>(g->m, 1u << 16);
-  k_sample_w<<<64, 256, 0, g->stream>>>(g->edges, g->m, g->wt == ADDS_F32, ns, d_sw);
-  CK(cudaMemcpyAsync(&sw, d_sw, 8, cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaStreamSynchronize(g->stream));
-  cudaFree(d_sw);
+  if (h[0]) return ADDS_ERR_INVALID;
+  double sw;
+  memcpy(&sw, h + 2, 8);
   g->avg_w = sw / ns;
+  g->sorted_valid = g->split_valid = false; /* the weight order changed */
+  ++g->wversion;
   return ADDS_OK;
 }
 
@@ -848,27 +853,22 @@ static int graph_sorted(adds_graph *g) {
     return ADDS_OK;
   }
   if (m >= 0x7FFFFFFFull) return ADDS_ERR_UNSUPPORTED;
-  uint32_t *buf = nullptr;
-  CK(cudaMalloc(&buf, m * 16));
-  uint32_t *wk = buf, *dv = buf + m, *wk2 = buf + 2 * m, *dv2 = buf + 3 * m;
+  if (!g->sort_buf) CK(cudaMalloc(&g->sort_buf, m * 16)); /* kept for re-sorts */
+  uint32_t *wk = g->sort_buf, *dv = wk + m, *wk2 = wk + 2 * m, *dv2 = wk + 3 * m;
   k_unzip<<<592, 256, 0, g->stream>>>(g->edges, m, wk, dv);
   size_t tb = 0;
   cub::DeviceSegmentedSort::SortPairs(nullptr, tb, wk, wk2, dv, dv2, (int)m, (int)g->n, g->row,
                                       g->row + 1, g->stream);
-  void *tmp = nullptr;
-  cudaError_t e = cudaMalloc(&tmp, tb ? tb : 1);
-  if (e != cudaSuccess) {
-    cudaFree(buf);
-    return cuda_fail(e, "sort temp");
+  if (tb > g->sort_tmp_bytes) {
+    if (g->sort_tmp) cudaFree(g->sort_tmp);
+    g->sort_tmp = nullptr;
+    g->sort_tmp_bytes = 0;
+    CK(cudaMalloc(&g->sort_tmp, tb));
+    g->sort_tmp_bytes = tb;
   }
-  e = cub::DeviceSegmentedSort::SortPairs(tmp, tb, wk, wk2, dv, dv2, (int)m, (int)g->n, g->row,
-                                          g->row + 1, g->stream);
-  if (e == cudaSuccess) {
-    k_zip<<<592, 256, 0, g->stream>>>(wk2, dv2, m, g->sedges);
-    e = cudaStreamSynchronize(g->stream);
-  }
-  cudaFree(tmp);
-  cudaFree(buf);
+  cudaError_t e = cub::DeviceSegmentedSort::SortPairs(g->sort_tmp, tb, wk, wk2, dv, dv2, (int)m,
+                                                      (int)g->n, g->row, g->row + 1, g->stream);
+  if (e == cudaSuccess) k_zip<<<592, 256, 0, g->stream>>>(wk2, dv2, m, g->sedges);
   if (e != cudaSuccess) return cuda_fail(e, "segmented sort");
   g->sorted_valid = true;
   g->split_valid = false;
@@ -895,7 +895,7 @@ static int graph_split(adds_graph *g, unsigned thr) {
     g->bytes += (size_t)g->n * 4;
   }
   k_split<<<592, 256, 0, g->stream>>>(g->row, g->sedges, g->n, thr, g->split);
-  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaGetLastError());
   g->split_thr = thr;
   g->split_valid = true;
   return ADDS_OK;
@@ -909,8 +909,12 @@ static int graph_layout(adds_graph *g, const Knobs &k, int shift, float scale,
     *split = nullptr;
     return ADDS_OK;
   }
+  const bool rebuild = !g->sorted_valid || !g->split_valid ||
+                       g->split_thr != light_threshold(g, shift, scale);
   const int rc = graph_split(g, light_threshold(g, shift, scale));
   if (rc) return rc;
+  /* the rebuild ran on the graph's stream; solves may run on another */
+  if (rebuild) CK(cudaStreamSynchronize(g->stream));
   *edges = g->sedges;
   *split = g->split;
   return ADDS_OK;
@@ -1115,9 +1119,12 @@ struct adds_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
   EngParams P;
   void *adj = nullptr; /* backward scratch (adjoint.cu) */
+  std::vector<unsigned long long> wversions; /* graph weight versions seen */
 };
 
 static int batch_engine(adds_batch *b) {
+  b->wversions.clear();
+  for (adds_graph *g : b->ugraph) b->wversions.push_back(g->wversion);
   std::vector<EngQuery> qv(b->qgraph.size());
   for (size_t i = 0; i < qv.size(); ++i) {
     adds_graph *g = b->qgraph[i];
@@ -1234,9 +1241,30 @@ static int batch_capture(adds_batch *b) {
   return ADDS_OK;
 }
 
+/* weights changed since the descriptors were built: the weight-sorted
+ * copies are rebuilt and the descriptors re-pointed (same sizing) */
+static int batch_relayout(adds_batch *b) {
+  bool changed = false;
+  for (size_t i = 0; i < b->ugraph.size(); ++i)
+    if (b->ugraph[i]->wversion != b->wversions[i]) changed = true;
+  if (!changed) return ADDS_OK;
+  for (size_t i = 0; i < b->qgraph.size(); ++i) {
+    const uint2 *edges;
+    const unsigned *split;
+    const int rc = graph_layout(b->qgraph[i], b->kn, b->shifts[i], b->scales[i], &edges, &split);
+    if (rc) return rc;
+    b->eng.qs_host[i].edges = edges;
+    b->eng.qs_host[i].split = split;
+  }
+  for (size_t i = 0; i < b->ugraph.size(); ++i) b->wversions[i] = b->ugraph[i]->wversion;
+  return engine_upload_queries(b->eng, b->stream);
+}
+
 extern "C" int adds_batch_launch(adds_batch *b) {
   if (!b) return ADDS_ERR_INVALID;
   CK(cudaSetDevice(b->device));
+  const int rl = batch_relayout(b);
+  if (rl) return rl;
   if (!b->captured) {
     int rc = batch_capture(b);
     if (rc) return rc;
@@ -1305,6 +1333,22 @@ extern "C" int adds_batch_set_sources(adds_batch *b, const uint32_t *srcs) {
 extern "C" int adds_batch_dist_ptr(adds_batch *b, uint32_t q, void **dptr) {
   if (!b || !dptr || q >= b->srcs.size()) return ADDS_ERR_INVALID;
   *dptr = b->dist_all + b->dist_off[q];
+  return ADDS_OK;
+}
+
+extern "C" int adds_batch_dist_all(adds_batch *b, void *out, uint64_t *offsets, uint64_t *total) {
+  if (!b) return ADDS_ERR_INVALID;
+  const size_t nq = b->srcs.size();
+  const size_t tot = b->dist_off[nq - 1] + b->qgraph[nq - 1]->n;
+  if (offsets)
+    for (size_t q = 0; q < nq; ++q) offsets[q] = b->dist_off[q];
+  if (total) *total = tot;
+  if (!out) return ADDS_OK;
+  CK(cudaSetDevice(b->device));
+  const bool dev = is_device_ptr(out);
+  CK(cudaMemcpyAsync(out, b->dist_all, tot * 4, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
   return ADDS_OK;
 }
 

@@ -267,7 +267,10 @@ enum : unsigned { ST_WORK = 0, ST_HUB = 1, ST_IDLE = 2, ST_EXIT = 3, ST_LOCAL = 
  * avail count, then the head index.  Returns the count, 0 if none. */
 __device__ __forceinline__ unsigned claim(SlotCtr *sc, long long av, const EngParams &P,
                                           unsigned long long *h0) {
-  const long long share = (long long)((P.nctas >> P.greed) ? (P.nctas >> P.greed) : 1u);
+  /* CTAs expected to share one query's bucket: all of them for a single
+   * solve, fewer as the batch has more queries */
+  const unsigned per_q = (P.nctas >> P.greed) / P.nq;
+  const long long share = (long long)(per_q ? per_q : 1u);
   long long want = (av + share - 1) / share;
   if (want > (long long)P.batch_max) want = P.batch_max;
   if (want < 1) want = 1;
@@ -614,7 +617,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
                      st_heavy = 0;
   /* per-phase SM cycle counts (thread 0's view; every phase ends at a
    * barrier, so thread 0 sees the CTA's time) */
-  unsigned long long cy_acq = 0, cy_load = 0, cy_edge = 0, cy_flush = 0, cy_idle = 0;
+  unsigned long long cy_acq = 0, cy_load = 0, cy_edge = 0, cy_flush = 0, cy_idle = 0,
+                     cy_mflush = 0, st_mflush = 0;
   const long long cy_start = clock64();
   long long cy_mark = cy_start;
 #define CY_LAP(acc)                     \
@@ -624,7 +628,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
     cy_mark = _n;                       \
   } while (0)
   if (tid == 0) {
-    S.cur_q = blockIdx.x % P.nq;
+    /* spread the CTAs evenly over the queries of a batch */
+    S.cur_q = (unsigned)(((unsigned long long)blockIdx.x * P.nq) / P.nctas) % P.nq;
     S.pcnt = 0;
     S.idle = 0;
     S.hungry = 0;
@@ -845,7 +850,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
         }
       }
       __syncthreads();
-      if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, S, d, deadline, st_pushes, false);
+      if (S.pcnt > FLUSH_AT) {
+        CY_LAP(cy_edge);
+        flush<BLOCK>(P, S, d, deadline, st_pushes, false);
+        CY_LAP(cy_mflush);
+        ++st_mflush;
+      }
     }
     __syncthreads();
     CY_LAP(cy_edge);
@@ -882,6 +892,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
         atomicAdd(&g->st_cyc[3], cy_flush);
         atomicAdd(&g->st_cyc[4], cy_idle);
         atomicAdd(&g->st_cyc[5], (unsigned long long)(clock64() - cy_start));
+        atomicAdd(&g->st_pad[0], cy_mflush);
+        atomicAdd(&g->st_pad[1], st_mflush);
         if (st_hub) atomicAdd(&g->st_hub, st_hub);
         if (st_local) atomicAdd(&g->st_local, st_local);
         if (st_hub_stale) atomicAdd(&g->st_hub_stale, st_hub_stale);
@@ -911,6 +923,7 @@ __global__ void init_kernel(EngParams P) {
       g->st_items = g->st_stale = g->st_edges = g->st_pushes = 0;
       g->st_batches = g->st_hub = g->st_local = g->st_hub_stale = g->st_heavy = 0;
       for (int i = 0; i < 6; ++i) g->st_cyc[i] = 0;
+      g->st_pad[0] = g->st_pad[1] = 0;
     }
     QueryCtl *c = d.ctl;
     c->ctrl = 0ull;

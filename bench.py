@@ -377,13 +377,202 @@ def run_reference(args, wl_name, wl, ws, rank, local):
     }
 
 
+def run_batched(args, ws, rank, local, dist):
+    """256 solves of uneven size in one persistent, graph-captured launch:
+    192 Erdos-Renyi graphs (n log-uniform in [1e3, 1e6], 8 draws per vertex,
+    int weights U[1,1000]) and 64 distinct sources on one R-MAT 20 graph.
+    Compared with a host loop of plain solves of the same queries."""
+    import adds_b200 as A
+    import torch
+    rng = np.random.default_rng(4096)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(1e6), size=192)).round().astype(int)
+    graphs, srcs = [], []
+    for i, n in enumerate(ns):
+        g = A.Graph.generate(A.gen_spec("er", n=int(n), edge_factor=8, wtype=0, w_lo=1,
+                                        w_hi=1000, seed=10_000 + i), local)
+        graphs.append(g)
+        srcs.append(int(rng.integers(0, g.n)))
+    r20 = A.Graph.generate(A.gen_spec("rmat", scale=20, wtype=0, w_lo=1, w_hi=1000, seed=20),
+                           local)
+    row = np.empty(r20.n + 1, dtype=np.uint64)
+    A.check(A.lib().adds_graph_download(r20.handle, row.ctypes.data, None, None))
+    cand = np.flatnonzero(np.diff(row) > 0)
+    rsrc = [int(x) for x in rng.choice(cand, size=64, replace=False)]
+    qg = graphs + [r20] * 64
+    qs = srcs + rsrc
+    opts = A.default_opts(timeout_ms=60000)
+    # the autotuner picks per-graph knobs on a representative member
+    if not args.no_tune:
+        r20.tune(rsrc[:2])
+        big = int(np.argmax(ns))
+        graphs[big].tune([srcs[big]])
+    b = A.Batch(qg, qs, opts)
+    for _ in range(args.warmup):
+        b.run()
+    torch.cuda.set_device(local)
+    barrier(dist, local)
+    torch.cuda.synchronize(local)
+    smi = ClockSampler(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else "/tmp", f"clocks_batched_rank{rank}.csv"))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    torch.cuda.synchronize(local)
+    kms = 0.0
+    for _ in range(args.steps):
+        b.launch()
+        st = b.sync()
+        kms += st["kernel_ms"]
+    ev1.record()
+    torch.cuda.synchronize(local)
+    clocks = smi.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    tmax, usum = reduce_max_sum(dist, local, elapsed, float(len(qs) * args.steps))
+    value = usum / tmax
+    # the same queries as a host loop of plain solves
+    for g, s in zip(qg, qs):
+        g.sssp_async(s, opts)
+    for g in set(qg):
+        g.sync()
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        for g, s in zip(qg, qs):
+            g.sssp_async(s, opts)
+        for g in set(qg):
+            g.sync()
+    loop_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    loop_solves_per_s = len(qs) / loop_s
+    # e2e: run through the C ABI and copy every distance array to pinned host memory
+    tot_n = int(b.layout()[1])
+    host = torch.empty(tot_n, dtype=torch.int32, pin_memory=True)
+    te0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        b.run()
+        b.dist_all(host.data_ptr())  # every query's distances, one copy
+    e2e_s = (time.perf_counter() - te0) / max(1, args.steps // 2)
+    out = {
+        "metric": "batched_sssp_solves_per_s", "value": value, "unit": "solves/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tmax / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "batched: 192 ER graphs (n log-uniform [1e3,1e6], 8 draws/vertex, "
+                               "U[1,1000]) + 64 sources on R-MAT 20, one graph-captured launch",
+                   "queries": len(qs), "vertices": tot_n, "parallelism": f"replicas{ws}"},
+        "loop_of_plain_solves_per_s": loop_solves_per_s,
+        "speedup_vs_loop": value / loop_solves_per_s,
+        "e2e": {"value": len(qs) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 4 * len(qs),
+                "d2h_bytes_per_step": 4 * tot_n},
+        "gpu_launches": 2 * args.steps, "clocks": clocks,
+        "extra": {"kernel_ms_per_launch": kms / args.steps},
+    }
+    b.close()
+    for g in graphs:
+        g.close()
+    r20.close()
+    return out
+
+
+def run_diff(args, ws, rank, local, dist):
+    """Differentiable batched SSSP: 128 grids (side log-uniform [64,512]),
+    w = softplus(theta), theta ~ N(0,1); 16 sources and 64 targets per grid;
+    L = sum c_t d(s,t), c_t ~ U(0,1).  A step is forward + backward."""
+    import torch
+
+    import adds_b200 as A
+    from adds_b200.autograd import batched_sssp
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(128)
+    sides = np.exp(rng.uniform(np.log(64), np.log(512), size=128)).round().astype(int)
+    graphs, thetas, targets, coefs = [], [], [], []
+    gen = torch.Generator(device="cuda").manual_seed(128)
+    for i, sd in enumerate(sides):
+        g = A.Graph.generate(A.gen_spec("plain_grid", side=int(sd), wtype=1, w_lo=1.0, w_hi=2.0,
+                                        seed=500 + i), local)
+        graphs.append(g)
+        thetas.append(torch.randn(g.m, generator=gen, device="cuda"))
+        t = torch.from_numpy(rng.choice(g.n, size=64, replace=False)).cuda()
+        targets.append(t)
+        coefs.append(torch.from_numpy(rng.uniform(0, 1, size=64).astype(np.float32)).cuda())
+    qg, qs, qi = [], [], []
+    for i, g in enumerate(graphs):
+        for s in rng.choice(g.n, size=16, replace=False):
+            qg.append(g)
+            qs.append(int(s))
+            qi.append(i)
+    for g, th in zip(graphs, thetas):  # set weights once so the tuner sees them
+        g.set_weights(torch.nn.functional.softplus(th).contiguous().data_ptr())
+    if not args.no_tune:
+        big = int(np.argmax(sides))
+        graphs[big].tune([qs[qi.index(big)]])
+    b = A.Batch(qg, qs, A.default_opts(timeout_ms=60000))
+    params = [th.clone().requires_grad_(True) for th in thetas]
+    off = torch.from_numpy(b.layout()[0].astype(np.int64)).cuda()
+    # flat indices of (query, target) pairs and their coefficients
+    gidx = torch.cat([off[q] + targets[qi[q]] for q in range(len(qg))])
+    gcoef = torch.cat([coefs[qi[q]] for q in range(len(qg))])
+
+    def step(backward=True):
+        w = [torch.nn.functional.softplus(p) for p in params]
+        flat = batched_sssp(b, graphs, w)
+        loss = (flat[gidx] * gcoef).sum()
+        if backward:
+            for p in params:
+                p.grad = None
+            loss.backward()
+        return loss
+
+    # where a step's time goes (outside the timed loops)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for g, p in zip(graphs, params):
+        g.set_weights(torch.nn.functional.softplus(p.detach()).contiguous().data_ptr())
+    t1 = time.perf_counter()
+    st = b.run()
+    t2 = time.perf_counter()
+    parts = {"set_weights_ms": (t1 - t0) * 1e3, "batch_run_ms": (t2 - t1) * 1e3,
+             "batch_kernel_ms": st["kernel_ms"], "items": st["items_popped"],
+             "edges": st["edges_scanned"]}
+
+    for _ in range(args.warmup):
+        step(True)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(False)
+    torch.cuda.synchronize(local)
+    fwd_s = (time.perf_counter() - t0) / args.steps
+    barrier(dist, local)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(True)
+    torch.cuda.synchronize(local)
+    fb_s = (time.perf_counter() - t0) / args.steps
+    tmax, usum = reduce_max_sum(dist, local, fb_s, 1.0)
+    out = {
+        "metric": "diff_sssp_fwd_bwd_per_s", "value": usum / tmax, "unit": "fwd+bwd/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "float32",
+        "data": "synthetic",
+        "config": {"workload": "diff: 128 grids (side log-uniform [64,512]), w=softplus(theta), "
+                               "16 sources x 64 targets per grid, L=sum c_t d(s,t)",
+                   "queries": len(qg), "parallelism": f"replicas{ws}"},
+        "fwd_ms": fwd_s * 1e3, "fwd_bwd_ms": fb_s * 1e3, "fwd_bwd_over_fwd": fb_s / fwd_s,
+        "gpu_launches": None, "parts": parts,
+    }
+    b.close()
+    for g in graphs:
+        g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS) + ["batched", "diff"])
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-tune", action="store_true")
@@ -392,6 +581,20 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_env()
+    if args.workload in ("batched", "diff"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no batched or differentiable path"}))
+            return
+        dist = dist_init(ws, local)
+        fn = run_batched if args.workload == "batched" else run_diff
+        out = fn(args, ws, rank, local, dist)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         if rank == 0:

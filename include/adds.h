@@ -94,6 +94,8 @@ typedef struct adds_stats {
   uint64_t heavy_lists;     /* settled vertices whose heavy edges were relaxed */
   uint64_t phase_cycles[6]; /* SM cycles summed over CTAs: acquire, load,
                                edges, flush, idle, total                      */
+  uint64_t mid_flush_cycles; /* of the edge phase: flushes of a full buffer   */
+  uint64_t mid_flushes;
   uint64_t reached;         /* vertices with finite distance (filled on request) */
   uint64_t reached_edges;   /* out-edges of reached vertices (filled on request) */
   int32_t delta_shift;      /* bucket shift at the end of the solve            */
@@ -194,6 +196,11 @@ int adds_batch_run(adds_batch *b, adds_stats *stats);
 int adds_batch_launch(adds_batch *b);
 int adds_batch_sync(adds_batch *b, adds_stats *stats);
 int adds_batch_dist(adds_batch *b, uint32_t q, void *dist_out);
+/* All queries' distances in one copy: query q occupies out[offsets[q] ..
+ * offsets[q] + n_q) (words; offsets are padded to 32-word multiples) and
+ * *total words are written.  out (host or device) may be NULL to only fill
+ * offsets (nq entries) and *total. */
+int adds_batch_dist_all(adds_batch *b, void *out, uint64_t *offsets, uint64_t *total);
 /* Device pointer to query q's distance array (valid until adds_batch_free). */
 int adds_batch_dist_ptr(adds_batch *b, uint32_t q, void **dptr);
 int adds_batch_set_sources(adds_batch *b, const uint32_t *srcs);
