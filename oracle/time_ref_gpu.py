@@ -1,0 +1,84 @@
+"""Times the reference ADDS GPU binary (oracle/_ref/, built by
+oracle/build_ref.sh) against this engine on one workload of bench.py.
+TEST/MEASUREMENT INFRASTRUCTURE ONLY.  Needs a GPU.
+
+  python oracle/time_ref_gpu.py rmat24 [nsources] [out.json]
+
+For each source, the reference binary runs as the reference's run_all.sh
+does (`sssp -s src -o out graph.gr 3>record`); its fd-3 record gives the
+average solve time over its RUN_LOOP (8 for int, 1 for float), whose timed
+region is the reference's own (kernel.cu:235-262).  GTEPS = out-edges of the
+reached vertices / time, for both.
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+import adds_b200 as A  # noqa: E402
+
+
+def main():
+    wl_name = sys.argv[1] if len(sys.argv) > 1 else "rmat24"
+    nsrc = int(sys.argv[2]) if len(sys.argv) > 2 else 2
+    out_json = sys.argv[3] if len(sys.argv) > 3 else None
+    wl = bench.WORKLOADS[wl_name]
+    g = bench.make_graph(wl, 0)
+    row = np.empty(g.n + 1, dtype=np.uint64)
+    A.check(A.lib().adds_graph_download(g.handle, row.ctypes.data, None, None))
+    srcs = bench.pick_sources(g, wl, row)[:nsrc]
+    binary = os.path.join(ROOT, "oracle", "_ref",
+                          "ads_int_sssp" if wl["wtype"] == 0 else "ads_float_sssp")
+    res = {"workload": wl_name, "n": g.n, "m": g.m, "sources": [], "binary": binary}
+    with tempfile.TemporaryDirectory() as tmp:
+        gr = os.path.join(tmp, wl_name + ".gr")
+        g.save_gr(gr)
+        for s in srcs:
+            g.sssp(s)
+            nr, mr = g.reached()
+            rec = os.path.join(tmp, "rec")
+            cmd = f'timeout 900 "{binary}" -s {s} "{gr}" 3>"{rec}" > "{tmp}/log" 2>&1'
+            r = subprocess.run(["bash", "-c", cmd])
+            if r.returncode != 0:
+                res["sources"].append({"src": s, "error": f"exit {r.returncode}",
+                                       "log_tail": open(os.path.join(tmp, "log")).read()[-800:]})
+                continue
+            name, ms, work = open(rec).read().split()
+            ref_ms = float(ms)
+            # this engine on the same graph and source, tuned first
+            best, _ = g.tune([s])
+            o = A.default_opts(timeout_ms=60000)
+            for _ in range(3):
+                g.sssp_async(s, o)
+            g.sync()
+            for _ in range(8):
+                g.sssp_async(s, o)
+            st = g.sync()
+            ours_ms = st["ms"] / 8
+            res["sources"].append({
+                "src": s, "m_r": mr, "n_r": nr, "ref_ms": ref_ms, "ref_work": int(work),
+                "ref_gteps": mr / ref_ms / 1e6, "ours_ms": ours_ms, "ours_gteps": mr / ours_ms / 1e6,
+                "speedup": ref_ms / ours_ms})
+            print(json.dumps(res["sources"][-1]), flush=True)
+    ok = [x for x in res["sources"] if "ref_ms" in x]
+    if ok:
+        res["ref_gteps_mean"] = float(np.mean([x["ref_gteps"] for x in ok]))
+        res["ours_gteps_mean"] = float(np.mean([x["ours_gteps"] for x in ok]))
+        res["speedup_mean"] = float(np.mean([x["speedup"] for x in ok]))
+    g.close()
+    txt = json.dumps(res, indent=1)
+    print(txt)
+    if out_json:
+        with open(out_json, "w") as f:
+            f.write(txt)
+
+
+if __name__ == "__main__":
+    main()

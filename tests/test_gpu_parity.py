@@ -113,3 +113,26 @@ def test_cli_int_matches_reference_text(tmp_path):
     assert open(out).read() == G.dist_text(ref, G.I32)
     name, ms, work = open(rec).read().split()
     assert name == "r12.gr" and float(ms) > 0 and int(work) > 0
+
+
+@pytest.mark.parametrize("name", ["ref_rmat16_int", "ref_rmat12_int", "ref_grid96_float"])
+def test_engine_matches_reference_adds_output(name):
+    """The engine against what the reference ADDS binary itself printed
+    (tests/golden/ref_*.npz, see tests/golden/make_ref_golden.py)."""
+    import gzip
+    import importlib.util
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("mrg", os.path.join(here, "make_ref_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    build, rule, binary = m.CASES[name]
+    g = build()
+    z = np.load(os.path.join(here, name + ".npz"))
+    dg = A.Graph.from_csr(g)
+    d, _ = dg.sssp(int(z["src"]), A.default_opts(**OPTS))
+    dg.close()
+    if binary == "ads_int_sssp":
+        assert np.array_equal(d, z["dist"])
+    else:
+        assert G.dist_text(d, G.F32) == gzip.decompress(z["text_gz"].tobytes()).decode()

@@ -1,9 +1,11 @@
 """CPU oracle: known answers, cross-checks, and the adjoint reference.
 
 The reference ships no golden vectors or known-answer tests for its path
-(its only check is a text diff against Galois Dijkstra output, verify.py),
-so the oracle is pinned here by hand-computed answers, by scipy's float64
-Dijkstra on integer graphs, and by the committed fixtures in tests/golden/.
+(its only check is a text diff against Galois Dijkstra output, verify.py).
+The oracle is pinned here by the reference's own output (the ADDS binaries
+built from the reference sources and run on a B200, fixtures ref_*.npz), by
+hand-computed answers, by scipy's float64 Dijkstra on integer graphs, and by
+frozen oracle outputs (oracle_golden.npz).
 """
 import os
 
@@ -179,3 +181,33 @@ def test_adjoint_zero_gap_ties_form_a_tree():
     assert [int(x) for x in e[1:]] == [0, 1, 3]
     # lambda: 3 -> 100, 2 -> 10 + 100, 1 -> 1 + 110
     assert grad.tolist() == [111.0, 110.0, 0.0, 100.0]
+
+
+def _ref_cases():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_ref_golden", os.path.join(HERE, "golden", "make_ref_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+@pytest.mark.parametrize("name", ["ref_rmat16_int", "ref_rmat12_int", "ref_grid96_float"])
+def test_oracle_pinned_to_reference_output(name):
+    """The fixtures hold what the reference ADDS binaries (built for sm_100a
+    by oracle/build_ref.sh, run on a B200 by tests/golden/make_ref_golden.py)
+    printed for these seeded graphs; the oracle must reproduce them exactly
+    (int: every distance; float: the reference's %f text)."""
+    import gzip
+    m = _ref_cases()
+    build, rule, binary = m.CASES[name]
+    g = build()
+    z = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    src = int(z["src"])
+    assert src == m.source_of(g, rule)
+    d, _ = O.dijkstra(g, src)
+    if binary == "ads_int_sssp":
+        assert np.array_equal(d, z["dist"])
+    else:
+        text = gzip.decompress(z["text_gz"].tobytes()).decode()
+        assert G.dist_text(d, G.F32) == text
