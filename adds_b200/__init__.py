@@ -154,6 +154,8 @@ class Graph:
     def tune(self, srcs, base: Opts | None = None):
         arr = (C.c_uint32 * len(srcs))(*srcs)
         best = Opts()
+        if base is not None:
+            best.engine = base.engine
         ms = C.c_double()
         check(lib().adds_tune(self._h, arr, len(srcs), C.byref(best), C.byref(ms)), "adds_tune")
         return best, ms.value

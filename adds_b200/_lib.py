@@ -55,7 +55,10 @@ class Opts(C.Structure):
         ("light_heavy", C.c_int32),
         ("block_threads", C.c_int32),
         ("greed", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("engine", C.c_int32),
+        ("group_ctas", C.c_int32),
+        ("solo_max", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -80,7 +83,11 @@ class Stats(C.Structure):
         ("delta_shift", C.c_int32),
         ("retries", C.c_int32),
         ("ctas", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("engine", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+        ("phases", C.c_uint64),
+        ("solo_phases", C.c_uint64),
+        ("repushes", C.c_uint64),
     ]
 
     def as_dict(self):

@@ -30,7 +30,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-Wall", "-I", os.path.join(ROOT, "include")]
-CU_SOURCES = ["engine.cu", "api.cu", "gen.cu", "adjoint.cu", "noalloc.cu"]
+CU_SOURCES = ["engine.cu", "phase.cu", "api.cu", "gen.cu", "adjoint.cu", "noalloc.cu"]
 CXX_SOURCES = ["grio.cpp"]
 
 
@@ -55,7 +55,8 @@ def build(force: bool = False, verbose: bool = False, extra_nvcc=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(BINDIR, exist_ok=True)
-    headers = [os.path.join(CSRC, "adds_internal.h"), os.path.join(ROOT, "include", "adds.h")]
+    headers = [os.path.join(CSRC, "adds_internal.h"), os.path.join(CSRC, "phase_internal.h"),
+               os.path.join(ROOT, "include", "adds.h")]
     jobs = []
     objs = []
     for src in CU_SOURCES:
@@ -80,7 +81,7 @@ def build(force: bool = False, verbose: bool = False, extra_nvcc=None) -> str:
     cli = os.path.join(CSRC, "sssp_cli.c")
     for name, defs in (("sssp_int", []), ("sssp_float", ["-DADDS_CLI_FLOAT"])):
         exe = os.path.join(BINDIR, name)
-        if force or _stale(exe, [cli, LIB, headers[1]]):
+        if force or _stale(exe, [cli, LIB, headers[-1]]):
             _run(["gcc", "-O2", "-std=c11", "-Wall", "-D_POSIX_C_SOURCE=200809L"] + defs +
                  ["-I", os.path.join(ROOT, "include"), cli, "-o", exe, "-L", LIBDIR, "-ladds",
                   "-Wl,-rpath,$ORIGIN/../lib"], verbose)

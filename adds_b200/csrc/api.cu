@@ -26,6 +26,7 @@
 
 #include "../../include/adds.h"
 #include "adds_internal.h"
+#include "phase_internal.h"
 
 /* engine.cu */
 cudaError_t adds_engine_prepare(bool flt, int block, int *max_blocks_per_sm);
@@ -93,6 +94,9 @@ extern "C" void adds_opts_init(adds_opts *o) {
   o->light_heavy = -1;
   o->block_threads = 0;
   o->greed = -1;
+  o->engine = ADDS_ENGINE_AUTO;
+  o->group_ctas = 0;
+  o->solo_max = -1;
 }
 
 static unsigned next_pow2(unsigned long long x) {
@@ -262,8 +266,28 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
+  int engine, variant, group_ctas, solo_max; /* phase engine */
   unsigned long long timeout_ns;
 };
+
+/* phase-engine kernel variant for (threads per CTA, CTAs per SM) */
+static int phase_variant(int block, int cps) {
+  if (block == 256) return cps == 2 ? 4 : 0;
+  if (block == 1024) return 2;
+  return cps == 1 ? 3 : 1;
+}
+
+static PhKnobs phase_knobs(const Knobs &k) {
+  PhKnobs p;
+  p.variant = k.variant;
+  p.ctas_per_sm = 0;
+  p.group_ctas = k.group_ctas;
+  p.hub_threshold = (unsigned)std::max(64, k.hub_threshold);
+  p.hub_chunk = 4096u;
+  p.solo_max = (unsigned)std::max(0, k.solo_max);
+  p.timeout_ns = k.timeout_ns;
+  return p;
+}
 
 static EngParams make_params(const Engine &E, const Knobs &k, unsigned single_src) {
   EngParams P;
@@ -373,6 +397,9 @@ struct adds_graph {
   double avg_deg = 0, avg_w = 0;
   size_t bytes = 0;
   Engine eng;
+  PhEngine peng;       /* phase engine (allocated on first use)            */
+  PhParams last_pp;
+  int last_engine = 0; /* engine of the solves in flight                   */
   unsigned grow = 1;
   int tuned = 0;
   adds_opts tuned_opts;
@@ -503,6 +530,7 @@ extern "C" void adds_graph_free(adds_graph *g) {
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   engine_free(g->eng);
+  ph_engine_free(g->peng);
   if (g->row) cudaFree(g->row);
   if (g->edges) cudaFree(g->edges);
   if (g->dist) cudaFree(g->dist);
@@ -804,8 +832,20 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   k->light_heavy = o->light_heavy >= 0 ? o->light_heavy : (t->light_heavy >= 0 ? t->light_heavy : 1);
   k->block = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 256);
   k->greed = o->greed >= 0 ? o->greed : (t->greed >= 0 ? t->greed : 4);
-  k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : 16384);
+  k->engine = o->engine > 0 ? o->engine : (t->engine > 0 ? t->engine : ADDS_ENGINE_PHASE);
+  if (k->engine != ADDS_ENGINE_ASYNC) k->engine = ADDS_ENGINE_PHASE;
+  const int hub_def = k->engine == ADDS_ENGINE_PHASE ? 4096 : 16384;
+  k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : hub_def);
   k->hub_chunk = 4096;
+  if (k->engine == ADDS_ENGINE_PHASE) {
+    const int pb = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 512);
+    const int pc = o->ctas_per_sm > 0 ? o->ctas_per_sm : (t->ctas_per_sm > 0 ? t->ctas_per_sm : 2);
+    k->variant = phase_variant(pb, pc);
+  } else {
+    k->variant = 0;
+  }
+  k->group_ctas = o->group_ctas > 0 ? o->group_ctas : (t->group_ctas > 0 ? t->group_ctas : 0);
+  k->solo_max = o->solo_max >= 0 ? o->solo_max : (t->solo_max >= 0 ? t->solo_max : 1024);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -943,6 +983,61 @@ static int graph_engine(adds_graph *g, const Knobs &k, int shift, float scale) {
   return engine_alloc(g->eng, g->device, g->wt == ADDS_F32, qv, g->grow, g->stream);
 }
 
+/* phase engine for plain solves of g (reused while the layout and the kernel
+ * variant stay the same) */
+static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float scale) {
+  const uint2 *edges;
+  const unsigned *split;
+  int rc = graph_layout(g, k, shift, scale, &edges, &split);
+  if (rc) return rc;
+  PhQuery q;
+  memset(&q, 0, sizeof q);
+  q.row = g->row;
+  q.edges = edges;
+  q.split = split;
+  q.dist = g->dist;
+  q.n = g->n;
+  q.src = 0;
+  q.scale = scale;
+  q.shift = (unsigned)shift;
+  q.m = g->m;
+  PhEngine &E = g->peng;
+  if (E.nq == 1 && E.variant == (unsigned)k.variant) {
+    PhQuery &h = E.qs_host[0];
+    if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)
+      return ADDS_OK;
+    E.qs_host[0] = q;
+    return ph_engine_upload(E, g->stream) ? ADDS_ERR_CUDA : ADDS_OK;
+  }
+  std::vector<PhQuery> qv(1, q);
+  rc = ph_engine_alloc(E, g->device, g->wt == ADDS_F32, qv, phase_knobs(k), g->grow, g->stream);
+  if (rc) {
+    snprintf(g_last_err, sizeof g_last_err, "phase engine allocation failed (%d)", rc);
+    ph_engine_free(E);
+  }
+  return rc;
+}
+
+static int phase_status(const PhEngine &E) { return ph_engine_status(E, g_last_err, sizeof g_last_err); }
+
+static void fill_phase_stats(const PhEngine &E, adds_stats *s) {
+  if (!s) return;
+  const PhGlobal &g = *E.g_host;
+  s->items_popped = g.st_items;
+  s->items_stale = g.st_stale;
+  s->edges_scanned = g.st_edges;
+  s->pushes = g.st_pushes;
+  s->batches = g.st_chunks;
+  s->hub_chunks = g.st_hub;
+  s->heavy_lists = g.st_heavy;
+  for (int i = 0; i < 4; ++i) s->phase_cycles[i] = g.st_cyc[i];
+  s->ctas = (int32_t)(E.groups * E.gsize);
+  s->engine = ADDS_ENGINE_PHASE;
+  s->phases = g.st_phases;
+  s->solo_phases = g.st_solo;
+  s->repushes = g.st_repush;
+}
+
 static cudaStream_t pick_stream(const adds_graph *g, const adds_opts *o) {
   return (o && o->stream) ? (cudaStream_t)o->stream : g->stream;
 }
@@ -954,12 +1049,12 @@ static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts) {
   float scale;
   Knobs k;
   resolve(g, opts, &k, &shift, &scale);
-  int rc = graph_engine(g, k, shift, scale);
+  const bool phase = k.engine == ADDS_ENGINE_PHASE;
+  int rc = phase ? graph_phase_engine(g, k, shift, scale) : graph_engine(g, k, shift, scale);
   if (rc) return rc;
   cudaStream_t st = pick_stream(g, opts);
-  EngParams P = make_params(g->eng, k, src);
   g->last_knobs = k;
-  g->last_params = P;
+  g->last_engine = k.engine;
   if (g->ring_used == adds_graph::kRing) { /* ring full: fold into nothing */
     CK(cudaStreamSynchronize(st));
     g->ring_used = 0;
@@ -968,7 +1063,17 @@ static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts) {
   for (int j = 0; j < 4; ++j)
     if (!ev[j]) CK(cudaEventCreate(&ev[j]));
   CK(cudaEventRecord(ev[0], st));
-  rc = engine_enqueue(g->eng, P, st, ev[1], ev[2]);
+  if (phase) {
+    PhParams P;
+    ph_engine_params(g->peng, phase_knobs(k), src, &P);
+    g->last_pp = P;
+    rc = ph_engine_enqueue(g->peng, P, st, ev[1], ev[2]);
+    if (rc) return cuda_fail(cudaGetLastError(), "phase engine launch");
+  } else {
+    EngParams P = make_params(g->eng, k, src);
+    g->last_params = P;
+    rc = engine_enqueue(g->eng, P, st, ev[1], ev[2]);
+  }
   if (rc) return rc;
   CK(cudaEventRecord(ev[3], st));
   ++g->ring_used;
@@ -1004,16 +1109,18 @@ extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds
     rc = sssp_enqueue(g, src, opts);
     if (rc) return rc;
     CK(cudaStreamSynchronize(st));
-    rc = engine_status(g->eng);
+    const bool phase = g->last_engine == ADDS_ENGINE_PHASE;
+    rc = phase ? phase_status(g->peng) : engine_status(g->eng);
     if (rc == ADDS_ERR_WL_OVERFLOW && retries < 4) {
       ++retries;
       g->grow *= 2;
-      engine_free(g->eng); /* re-allocated at the larger size on the rerun */
+      /* re-allocated at the larger size on the rerun */
+      if (phase) ph_engine_free(g->peng); else engine_free(g->eng);
       g->ring_used = 0;
       continue;
     }
     if (rc) {
-      engine_full_reset(g->eng, st);
+      if (phase) ph_engine_reset(g->peng, st); else engine_full_reset(g->eng, st);
       g->ring_used = 0;
       return rc;
     }
@@ -1025,8 +1132,14 @@ extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds
     memset(stats, 0, sizeof *stats);
     stats->ms = ms;
     stats->kernel_ms = kms;
-    fill_stats(g->eng, g->last_params, stats);
-    stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+    if (g->last_engine == ADDS_ENGINE_PHASE) {
+      fill_phase_stats(g->peng, stats);
+      stats->delta_shift = (int32_t)g->peng.qs_host[0].shift;
+    } else {
+      fill_stats(g->eng, g->last_params, stats);
+      stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+      stats->engine = ADDS_ENGINE_ASYNC;
+    }
     stats->retries = retries;
   }
   g->pending = 0;
@@ -1052,19 +1165,26 @@ extern "C" int adds_graph_sync(adds_graph *g, adds_stats *stats) {
   CK(cudaStreamSynchronize(g->stream));
   double ms = 0, kms = 0;
   ring_times(g, &ms, &kms);
-  if (g->eng.nq == 0) return ADDS_OK;
-  rc = engine_status(g->eng);
+  const bool phase = g->last_engine == ADDS_ENGINE_PHASE;
+  if (phase ? g->peng.nq == 0 : g->eng.nq == 0) return ADDS_OK;
+  rc = phase ? phase_status(g->peng) : engine_status(g->eng);
   g->pending = 0;
   if (rc) {
-    engine_full_reset(g->eng, g->stream);
+    if (phase) ph_engine_reset(g->peng, g->stream); else engine_full_reset(g->eng, g->stream);
     return rc;
   }
   if (stats) {
     memset(stats, 0, sizeof *stats);
     stats->ms = ms;
     stats->kernel_ms = kms;
-    fill_stats(g->eng, g->last_params, stats);
-    stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+    if (phase) {
+      fill_phase_stats(g->peng, stats);
+      stats->delta_shift = (int32_t)g->peng.qs_host[0].shift;
+    } else {
+      fill_stats(g->eng, g->last_params, stats);
+      stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+      stats->engine = ADDS_ENGINE_ASYNC;
+    }
   }
   return ADDS_OK;
 }
@@ -1110,6 +1230,8 @@ struct adds_batch {
   unsigned *dist_all = nullptr;
   std::vector<size_t> dist_off;
   Engine eng;
+  PhEngine peng; /* used when kn.engine is ADDS_ENGINE_PHASE */
+  PhParams pp;
   unsigned grow = 1;
   Knobs kn;
   std::vector<int> shifts;
@@ -1122,9 +1244,47 @@ struct adds_batch {
   std::vector<unsigned long long> wversions; /* graph weight versions seen */
 };
 
+static int batch_phase_engine(adds_batch *b) {
+  std::vector<PhQuery> qv(b->qgraph.size());
+  for (size_t i = 0; i < qv.size(); ++i) {
+    adds_graph *g = b->qgraph[i];
+    const uint2 *edges;
+    const unsigned *split;
+    const int rc = graph_layout(g, b->kn, b->shifts[i], b->scales[i], &edges, &split);
+    if (rc) return rc;
+    PhQuery q;
+    memset(&q, 0, sizeof q);
+    q.row = g->row;
+    q.edges = edges;
+    q.split = split;
+    q.dist = b->dist_all + b->dist_off[i];
+    q.n = g->n;
+    q.src = b->srcs[i];
+    q.scale = b->scales[i];
+    q.shift = (unsigned)b->shifts[i];
+    q.m = g->m;
+    qv[i] = q;
+  }
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  b->captured = false;
+  const PhKnobs pk = phase_knobs(b->kn);
+  int rc = ph_engine_alloc(b->peng, b->device, b->flt, qv, pk, b->grow, b->stream);
+  if (rc) {
+    snprintf(g_last_err, sizeof g_last_err, "phase engine allocation failed (%d)", rc);
+    ph_engine_free(b->peng);
+    return rc;
+  }
+  ph_engine_params(b->peng, pk, 0xFFFFFFFFu, &b->pp);
+  return ADDS_OK;
+}
+
 static int batch_engine(adds_batch *b) {
   b->wversions.clear();
   for (adds_graph *g : b->ugraph) b->wversions.push_back(g->wversion);
+  if (b->kn.engine == ADDS_ENGINE_PHASE) return batch_phase_engine(b);
   std::vector<EngQuery> qv(b->qgraph.size());
   for (size_t i = 0; i < qv.size(); ++i) {
     adds_graph *g = b->qgraph[i];
@@ -1213,6 +1373,7 @@ extern "C" void adds_batch_free(adds_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   engine_free(b->eng);
+  ph_engine_free(b->peng);
   if (b->dist_all) cudaFree(b->dist_all);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -1227,7 +1388,9 @@ extern "C" void adds_batch_free(adds_batch *b) {
 static int batch_capture(adds_batch *b) {
   cudaGraph_t gr = nullptr;
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = engine_enqueue(b->eng, b->P, b->stream, b->k0, b->k1);
+  int rc = b->kn.engine == ADDS_ENGINE_PHASE
+               ? (ph_engine_enqueue(b->peng, b->pp, b->stream, b->k0, b->k1) ? ADDS_ERR_CUDA : ADDS_OK)
+               : engine_enqueue(b->eng, b->P, b->stream, b->k0, b->k1);
   cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
   if (rc || e != cudaSuccess) {
     if (gr) cudaGraphDestroy(gr);
@@ -1253,10 +1416,17 @@ static int batch_relayout(adds_batch *b) {
     const unsigned *split;
     const int rc = graph_layout(b->qgraph[i], b->kn, b->shifts[i], b->scales[i], &edges, &split);
     if (rc) return rc;
-    b->eng.qs_host[i].edges = edges;
-    b->eng.qs_host[i].split = split;
+    if (b->kn.engine == ADDS_ENGINE_PHASE) {
+      b->peng.qs_host[i].edges = edges;
+      b->peng.qs_host[i].split = split;
+    } else {
+      b->eng.qs_host[i].edges = edges;
+      b->eng.qs_host[i].split = split;
+    }
   }
   for (size_t i = 0; i < b->ugraph.size(); ++i) b->wversions[i] = b->ugraph[i]->wversion;
+  if (b->kn.engine == ADDS_ENGINE_PHASE)
+    return ph_engine_upload(b->peng, b->stream) ? ADDS_ERR_CUDA : ADDS_OK;
   return engine_upload_queries(b->eng, b->stream);
 }
 
@@ -1279,7 +1449,8 @@ extern "C" int adds_batch_sync(adds_batch *b, adds_stats *stats) {
   if (!b) return ADDS_ERR_INVALID;
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
-  int rc = engine_status(b->eng);
+  const bool phase = b->kn.engine == ADDS_ENGINE_PHASE;
+  int rc = phase ? phase_status(b->peng) : engine_status(b->eng);
   if (rc) return rc;
   if (stats) {
     memset(stats, 0, sizeof *stats);
@@ -1288,7 +1459,12 @@ extern "C" int adds_batch_sync(adds_batch *b, adds_stats *stats) {
     CK(cudaEventElapsedTime(&kms, b->k0, b->k1));
     stats->ms = ms;
     stats->kernel_ms = kms;
-    fill_stats(b->eng, b->P, stats);
+    if (phase) {
+      fill_phase_stats(b->peng, stats);
+    } else {
+      fill_stats(b->eng, b->P, stats);
+      stats->engine = ADDS_ENGINE_ASYNC;
+    }
     stats->delta_shift = b->shifts.empty() ? 0 : b->shifts[0];
   }
   return ADDS_OK;
@@ -1309,7 +1485,8 @@ extern "C" int adds_batch_run(adds_batch *b, adds_stats *stats) {
       continue;
     }
     if (rc) {
-      engine_full_reset(b->eng, b->stream);
+      if (b->kn.engine == ADDS_ENGINE_PHASE) ph_engine_reset(b->peng, b->stream);
+      else engine_full_reset(b->eng, b->stream);
       return rc;
     }
     if (stats) stats->retries = retries;
@@ -1323,10 +1500,12 @@ extern "C" int adds_batch_set_sources(adds_batch *b, const uint32_t *srcs) {
     if (srcs[i] >= b->qgraph[i]->n) return ADDS_ERR_INVALID;
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
-  for (size_t i = 0; i < b->srcs.size(); ++i) {
-    b->srcs[i] = srcs[i];
-    b->eng.qs_host[i].src = srcs[i];
+  for (size_t i = 0; i < b->srcs.size(); ++i) b->srcs[i] = srcs[i];
+  if (b->kn.engine == ADDS_ENGINE_PHASE) {
+    for (size_t i = 0; i < b->srcs.size(); ++i) b->peng.qs_host[i].src = srcs[i];
+    return ph_engine_upload(b->peng, b->stream) ? ADDS_ERR_CUDA : ADDS_OK;
   }
+  for (size_t i = 0; i < b->srcs.size(); ++i) b->eng.qs_host[i].src = srcs[i];
   return engine_upload_queries(b->eng, b->stream);
 }
 
@@ -1423,6 +1602,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   g->tuned = 0;
   adds_opts cur;
   adds_opts_init(&cur);
+  if (best && best->engine > 0) cur.engine = best->engine; /* in: engine to tune */
   Knobs k;
   int s0;
   float sc;
@@ -1437,6 +1617,8 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   cur.light_heavy = k.light_heavy;
   cur.block_threads = k.block;
   cur.greed = k.greed;
+  cur.engine = k.engine;
+  cur.solo_max = k.solo_max;
   double bm = time_solves(g, srcs, ns, &cur);
   auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
     for (int v : vals) {
@@ -1454,6 +1636,37 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   for (int d = -4; d <= 4; ++d)
     if (s0 + d >= 0 && s0 + d <= 31) shifts.push_back(s0 + d);
   try_field(&adds_opts::delta_shift, shifts);
+  if (k.engine == ADDS_ENGINE_PHASE) {
+    /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
+    const int combos[5][2] = {{512, 2}, {256, 4}, {1024, 1}, {512, 1}, {256, 2}};
+    for (const auto &cb : combos) {
+      adds_opts t = cur;
+      t.block_threads = cb[0];
+      t.ctas_per_sm = cb[1];
+      if (t.block_threads == cur.block_threads && t.ctas_per_sm == cur.ctas_per_sm) continue;
+      const double ms = time_solves(g, srcs, ns, &t);
+      if (ms < bm * 0.98) {
+        bm = ms;
+        cur = t;
+      }
+    }
+    try_field(&adds_opts::solo_max, {0, 256, 512, 1024, 2048, 4096});
+    try_field(&adds_opts::hub_threshold, {1024, 4096, 16384});
+    try_field(&adds_opts::light_heavy, {0, 1});
+    if (cur.delta_shift != s0) {
+      std::vector<int> s2;
+      for (int d = -1; d <= 1; ++d)
+        if (cur.delta_shift + d >= 0 && cur.delta_shift + d <= 31) s2.push_back(cur.delta_shift + d);
+      try_field(&adds_opts::delta_shift, s2);
+    }
+    if (bm >= 1e29) return ADDS_ERR_DEVICE_TIMEOUT;
+    g->tuned_opts = cur;
+    g->tuned_opts.stream = nullptr;
+    g->tuned = 1;
+    if (best) *best = g->tuned_opts;
+    if (best_ms) *best_ms = bm / ns;
+    return ADDS_OK;
+  }
   try_field(&adds_opts::window, {1, 2, 3, 4, 8});
   try_field(&adds_opts::batch_max, {64, 128, 256, 512});
   try_field(&adds_opts::hub_threshold, {4096, 16384, 65536});

@@ -1,0 +1,1019 @@
+/*
+ * phase.cu — bulk-synchronous bucketed delta-stepping SSSP for sm_100a.
+ *
+ * Behavioural source: ADDS (ads_int/kernel.cu:30-128 relaxation,
+ * ads_int/wl.h:192-1972 bucket worklist).  Kept from the reference:
+ *   - circular distance buckets, bucket = key >> shift (wl.h:1958-1972),
+ *     the farthest slot collecting everything beyond the ring;
+ *   - relax new = d[u] + w, accept if d[v] > new, atomicMin, push
+ *     (kernel.cu:112-121); float relaxes fl(d[u] + w) with a 32-bit
+ *     atomicMin on the bits of the non-negative float instead of the
+ *     reference's 64-bit CAS (ads_float/csr_graph.h:58-70);
+ *   - long rows split across workers (tb_coop_assign, wl.h:1638-1696; here
+ *     across every CTA of the group);
+ *   - the reference's per-thread work counts (wl.h:1835-1839) as statistics.
+ * Different: the buckets are settled in phases (Meyer-Sanders light/heavy
+ * delta-stepping).  A group of CTAs expands one frontier, meets at a group
+ * barrier, and the last CTA to arrive decides the next frontier from the list
+ * tails; while frontiers are small that CTA keeps running them alone with
+ * block barriers only.  There is no manager block, no CDP launch and no
+ * per-push fence; every wait is bounded by a device deadline and reports
+ * an error word instead of trapping.
+ *
+ * Batches: every group takes queries from a shared counter (largest first)
+ * and solves each one start to finish, distance initialisation included, so
+ * a batch of uneven solves is one launch.
+ */
+#include <cuda_runtime.h>
+
+#include "phase_internal.h"
+
+namespace adds_phase {
+
+#define PH_M_START 5u /* bootstrap pseudo-phase: nothing ran yet */
+
+/* ------------------------------------------------------------------------ */
+/* memory-model helpers (PTX ISA: ld/st .relaxed/.acquire/.release .gpu)     */
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned long long ld_rlx64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_rlx32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acq32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_rlx64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_rlx32(unsigned *p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+/* L2 policy for the edge stream: each edge is read about once per solve, so
+ * its lines go first and the distance array keeps its place in L2. */
+__device__ __forceinline__ unsigned long long evict_first_policy() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint2 ld_edge(const uint2 *p, unsigned long long pol) {
+  uint2 r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+      : "=r"(r.x), "=r"(r.y)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
+enum : unsigned { W_BARRIER = 1, W_PT = 2, W_ALLOC = 3, W_MAPPING = 4, W_HUB = 5 };
+
+__device__ __forceinline__ void raise_err(PhGlobal *g, unsigned code, unsigned where) {
+  if (atomicCAS(&g->err, 0u, code) == 0u) st_rlx32(&g->err_where, where);
+}
+
+/* Bounded wait: call once per spin iteration; false = give up. */
+struct Waiter {
+  unsigned long long deadline;
+  unsigned it;
+  __device__ __forceinline__ bool spin(PhGlobal *g, unsigned where, unsigned sleep_cap) {
+    ++it;
+    if ((it & 15u) == 0u) {
+      if (ld_rlx32(&g->err) != 0u) return false;
+      if (gtimer() > deadline) {
+        raise_err(g, PH_ERR_TIMEOUT, where);
+        return false;
+      }
+    }
+    __nanosleep(it < 32 ? 32 : sleep_cap);
+    return true;
+  }
+};
+
+/* ------------------------------------------------------------------------ */
+/* bucket mapping (dist_to_bag_id_int, wl.h:1958-1972)                        */
+template <bool FLT>
+__device__ __forceinline__ unsigned bucket_of(unsigned d, float scale, unsigned shift) {
+  unsigned key = d;
+  if (FLT) key = __float2uint_rz(__fmul_rn(__uint_as_float(d), scale));
+  return key >> shift;
+}
+/* list of a push with bucket b relative to the base bucket being settled */
+__device__ __forceinline__ unsigned route(unsigned b, unsigned base) {
+  if (b <= base) return PH_LNEXT;
+  const unsigned off = min(b - base, (unsigned)PH_NSLOT - 1u);
+  return (base + off) & (PH_NSLOT - 1u);
+}
+
+/* ------------------------------------------------------------------------ */
+/* shared memory of one CTA                                                   */
+#define PH_RES_PAGES 4u /* pages one list reservation may touch (flush size) */
+
+template <int BLOCK>
+struct PSmem {
+  static constexpr int U = 4;                     /* edges per thread per round */
+  static constexpr int SB = 2 * BLOCK * U + BLOCK; /* staged pushes             */
+  static_assert(SB <= (int)((PH_RES_PAGES - 1u) * PH_PAGE + 1u),
+                "a flush must fit in PH_RES_PAGES pages of one list");
+  unsigned it_rb[BLOCK];                          /* first edge of each item    */
+  unsigned it_du[BLOCK];                          /* distance of each item      */
+  unsigned it_off[BLOCK];                         /* exclusive scan of degrees  */
+  unsigned pb_v[SB];
+  unsigned pb_d[SB];
+  unsigned short pb_rank[SB];
+  unsigned char pb_l[SB];
+  unsigned hist[PH_NLIST];
+  unsigned bpg[PH_NLIST][PH_RES_PAGES]; /* pages of each list's reservation  */
+  unsigned long long bbase[PH_NLIST];
+  unsigned long long ptc_vp[PH_NLIST]; /* per-list page-table cache           */
+  unsigned ptc_pi[PH_NLIST];
+  unsigned wsum[BLOCK / 32];
+  PhDesc D;                            /* the phase being run                 */
+  unsigned long long st_items, st_stale, st_heavy, st_repush, st_pushes, st_chunks, st_hubs,
+      st_solo;
+  unsigned long long claim;
+  unsigned total, pcnt, leader, gen, pi0, pi1, stop;
+};
+
+/* what a CTA keeps for the kernel's lifetime; the group's arrays are
+ * recomputed from the parameters where they are used */
+struct Ctx {
+  unsigned gi, rank;
+  unsigned long long deadline;
+  unsigned edges; /* per-thread count; the rest is counted in shared memory */
+};
+__device__ __forceinline__ PhGroup *grp_of(const PhParams &P, const Ctx &c) { return P.grp + c.gi; }
+
+__device__ __forceinline__ unsigned long long *pt_cell(const PhParams &P, const Ctx &c, unsigned L,
+                                                       unsigned long long vp) {
+  return P.pt + ((((unsigned long long)c.gi * PH_NLIST + L) << P.ptn_log2) |
+                 (vp & ((1ull << P.ptn_log2) - 1ull)));
+}
+__device__ __forceinline__ unsigned long long *entry_ptr(const PhParams &P, const Ctx &c,
+                                                         unsigned page, unsigned long long idx) {
+  return P.pool + ((((unsigned long long)c.gi * P.pages_per_group + page) << PH_PAGE_LOG2) |
+                   (idx & (PH_PAGE - 1u)));
+}
+__device__ __forceinline__ PhHub *hub_of(const PhParams &P, const Ctx &c) {
+  return P.hub + (unsigned long long)c.gi * P.hub_cap;
+}
+
+/* Page of virtual page vp of list L; waits for the reservation that owns the
+ * page's first entry to map it (a bounded, short wait: that reservation is
+ * in flight in the same phase). */
+__device__ unsigned pt_wait(const PhParams &P, const Ctx &c, unsigned L, unsigned long long vp,
+                            unsigned long long *cvp, unsigned *cpi) {
+  if (*cvp == vp) return *cpi;
+  unsigned long long *cell = pt_cell(P, c, L, vp);
+  Waiter w{c.deadline, 0};
+  for (;;) {
+    const unsigned long long e = ld_rlx64(cell);
+    if ((unsigned)e == (unsigned)vp) {
+      *cvp = vp;
+      *cpi = (unsigned)(e >> 32);
+      return *cpi;
+    }
+    if (!w.spin(P.g, W_PT, 64)) return 0xFFFFFFFFu;
+  }
+}
+
+/* Reserves cnt entries at the tail of list L and maps the pages the range
+ * touches (at most PH_RES_PAGES) into pgs[].  The reservation holding a
+ * page's first entry takes a page from the group's bump counter; it maps the
+ * pages it owns before it waits for the first one, so a later reservation
+ * never waits behind its wait.  Replaces push_work's reservation and
+ * address translation (wl.h:1854-1928). */
+__device__ bool list_reserve(const PhParams &P, const Ctx &c, unsigned L, unsigned cnt,
+                             unsigned long long *pbase, unsigned *pgs,
+                             unsigned long long *cvp, unsigned *cpi) {
+  PhGroup *G = grp_of(P, c);
+  const unsigned long long base = atomicAdd(&G->tails[L].tail, (unsigned long long)cnt);
+  *pbase = base;
+  const unsigned long long vp0 = base >> PH_PAGE_LOG2;
+  const unsigned long long vp1 = (base + cnt - 1ull) >> PH_PAGE_LOG2;
+  for (unsigned j = 0; j < PH_RES_PAGES; ++j) pgs[j] = 0xFFFFFFFFu;
+  if (vp1 - vp0 >= PH_RES_PAGES) { /* larger than any flush: engine fault */
+    raise_err(P.g, PH_ERR_MAPPING, W_ALLOC);
+    return false;
+  }
+  for (unsigned long long vp = vp1 + 1ull; vp-- > vp0;) {
+    if ((vp << PH_PAGE_LOG2) < base) continue;
+    const unsigned pg = atomicAdd(&G->page_next, 1u);
+    if (pg >= P.pages_per_group) {
+      raise_err(P.g, PH_ERR_OVERFLOW, W_ALLOC);
+      return false;
+    }
+    st_rlx64(pt_cell(P, c, L, vp), ((unsigned long long)pg << 32) | (unsigned)vp);
+    *cvp = vp;
+    *cpi = pg;
+    pgs[vp - vp0] = pg;
+  }
+  if ((vp0 << PH_PAGE_LOG2) < base) { /* first page: mapped by an earlier reservation */
+    const unsigned pg = pt_wait(P, c, L, vp0, cvp, cpi);
+    if (pg == 0xFFFFFFFFu) return false;
+    pgs[0] = pg;
+  }
+  return true;
+}
+
+/* Page of an entry already written in an earlier phase (its mapping is
+ * visible after the barrier; a missing one is an engine fault). */
+__device__ __forceinline__ unsigned pt_lookup(const PhParams &P, const Ctx &c, unsigned L,
+                                              unsigned long long vp) {
+  const unsigned long long e = ld_rlx64(pt_cell(P, c, L, vp));
+  if ((unsigned)e != (unsigned)vp) {
+    raise_err(P.g, PH_ERR_MAPPING, W_MAPPING);
+    return 0xFFFFFFFFu;
+  }
+  return (unsigned)(e >> 32);
+}
+
+/* ------------------------------------------------------------------------ */
+/* staging and flushing of pushes                                             */
+template <int BLOCK>
+__device__ __forceinline__ void stage(PSmem<BLOCK> &S, unsigned v, unsigned d, unsigned L) {
+  const unsigned mask = __activemask();
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned leader = __ffs(mask) - 1u;
+  unsigned pos = 0;
+  if (lane == leader) pos = atomicAdd(&S.pcnt, (unsigned)__popc(mask));
+  pos = __shfl_sync(mask, pos, leader) + __popc(mask & ((1u << lane) - 1u));
+  S.pb_v[pos] = v;
+  S.pb_d[pos] = d;
+  S.pb_l[pos] = (unsigned char)L;
+}
+
+/* Counting sort of the staged pushes by list, one reservation per list, the
+ * entry stores.  Nothing else: the phase barrier publishes them.  Replaces the
+ * per-warp reservation + st.cg + __threadfence + write_done update of
+ * push_work (wl.h:1902-1928).  Call with every thread, after a barrier. */
+template <int BLOCK>
+__device__ void flush(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
+  const unsigned tid = threadIdx.x;
+  const unsigned cnt = S.pcnt;
+  if (cnt == 0u) return;
+  if (tid < PH_NLIST) S.hist[tid] = 0u;
+  __syncthreads();
+  for (unsigned i = tid; i < cnt; i += BLOCK)
+    S.pb_rank[i] = (unsigned short)atomicAdd(&S.hist[S.pb_l[i]], 1u);
+  __syncthreads();
+  if (tid < PH_NLIST) {
+    const unsigned h = S.hist[tid];
+    if (h != 0u) {
+      unsigned long long b;
+      unsigned pg[PH_RES_PAGES];
+      list_reserve(P, c, tid, h, &b, pg, &S.ptc_vp[tid], &S.ptc_pi[tid]);
+      S.bbase[tid] = b;
+      for (unsigned j = 0; j < PH_RES_PAGES; ++j) S.bpg[tid][j] = pg[j];
+    }
+  }
+  __syncthreads();
+  for (unsigned i = tid; i < cnt; i += BLOCK) {
+    const unsigned L = S.pb_l[i];
+    const unsigned long long b = S.bbase[L];
+    const unsigned long long idx = b + S.pb_rank[i];
+    const unsigned pg = S.bpg[L][(idx >> PH_PAGE_LOG2) - (b >> PH_PAGE_LOG2)];
+    if (pg != 0xFFFFFFFFu)
+      st_rlx64(entry_ptr(P, c, pg, idx), ((unsigned long long)S.pb_d[i] << 32) | S.pb_v[i]);
+  }
+  if (tid == 0u) S.st_pushes += cnt;
+  __syncthreads();
+  if (tid == 0u) S.pcnt = 0u;
+  __syncthreads();
+}
+
+/* block-wide exclusive scan of one value per thread */
+template <int BLOCK>
+__device__ __forceinline__ unsigned block_exscan(PSmem<BLOCK> &S, unsigned x, unsigned &total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  if (lane == 31u) S.wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned w = lane < BLOCK / 32 ? S.wsum[lane] : 0u;
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= (unsigned)o) wi += y;
+    }
+    if (lane < BLOCK / 32) S.wsum[lane] = wi - w;
+    if (lane == 31u) S.total = wi;
+  }
+  __syncthreads();
+  total = S.total;
+  return S.wsum[warp] + incl - x;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Edge-balanced expansion of the k items staged in S.it_* (E edges in all):
+ * relax, atomicMin, stage the winners.  Each thread takes every BLOCK-th edge
+ * of a round of BLOCK*U, so loads of consecutive threads are consecutive in
+ * memory; the next round's edge loads are issued before this round's
+ * distance gathers and atomics, so the edge stream stays in flight. */
+template <bool FLT, int BLOCK>
+__device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, const PhQuery &Q, unsigned k,
+                       unsigned E, unsigned base) {
+  constexpr int U = PSmem<BLOCK>::U;
+  constexpr unsigned R = BLOCK * U;
+  constexpr unsigned FLUSH_AT = PSmem<BLOCK>::SB - R - BLOCK;
+  const unsigned tid = threadIdx.x;
+  const uint2 *__restrict__ edges = Q.edges;
+  unsigned *dist = Q.dist;
+  const float scale = Q.scale;
+  const unsigned shift = Q.shift;
+  const unsigned long long pol = evict_first_policy();
+  int lo = 0; /* a thread's edges only move forward: searches start at the last item */
+  uint2 ne[U];
+  unsigned nu[U];
+  auto load_round = [&](unsigned eb) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned e = eb + u * BLOCK + tid;
+      nu[u] = 0xFFFFFFFFu;
+      ne[u] = make_uint2(0u, 0u);
+      if (e < E) {
+        int hi = (int)k - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (S.it_off[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        ne[u] = ld_edge(edges + S.it_rb[lo] + (e - S.it_off[lo]), pol);
+        nu[u] = S.it_du[lo];
+      }
+    }
+  };
+  if (E) load_round(0);
+  unsigned nedges = 0;
+  for (unsigned eb = 0; eb < E; eb += R) {
+    uint2 ce[U];
+    unsigned nd[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ce[u] = ne[u];
+      const unsigned du = nu[u];
+      nd[u] = 0xFFFFFFFFu;
+      if (du != 0xFFFFFFFFu) {
+        nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(ce[u].y)))
+                    : du + ce[u].y;
+        ++nedges;
+      }
+    }
+    if (eb + R < E) load_round(eb + R);
+    unsigned cur[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + ce[u].x) : 0u;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (nd[u] < cur[u]) {
+        const unsigned old = atomicMin(dist + ce[u].x, nd[u]);
+        if (old > nd[u]) stage<BLOCK>(S, ce[u].x, nd[u], route(bucket_of<FLT>(nd[u], scale, shift), base));
+      }
+    }
+    __syncthreads();
+    if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, c, S);
+  }
+  c.edges += nedges;
+}
+
+/* ------------------------------------------------------------------------ */
+/* One phase (or, solo, the whole of it on this CTA).                         */
+template <bool FLT, int BLOCK>
+__device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, bool solo) {
+  const unsigned tid = threadIdx.x;
+  const unsigned mode = S.D.mode;
+  if (mode == PH_M_START || mode == PH_M_EXIT) return;
+  PhGroup *G = grp_of(P, c);
+  const PhQuery &Q = P.qs[S.D.q];
+  const unsigned long long d_lo = S.D.lo, d_hi = S.D.hi, d_wb = S.D.work_base;
+  const unsigned d_base = S.D.base, d_list = S.D.list;
+  const unsigned rank = solo ? 0u : c.rank;
+  const unsigned gsize = solo ? 1u : P.gsize;
+  if (mode == PH_M_INIT) {
+    const unsigned inf = P.is_float ? 0x7F7FFFFFu : 0x7FFFFFFFu;
+    if ((reinterpret_cast<unsigned long long>(Q.dist) & 15ull) == 0ull) {
+      uint4 *d4 = reinterpret_cast<uint4 *>(Q.dist);
+      const unsigned n4 = Q.n >> 2;
+      const uint4 x = make_uint4(inf, inf, inf, inf);
+      for (unsigned i = rank * BLOCK + tid; i < n4; i += gsize * BLOCK) __stcg(d4 + i, x);
+      if (rank == 0u && tid < (Q.n & 3u)) __stcg(Q.dist + (n4 << 2) + tid, inf);
+    } else {
+      for (unsigned i = rank * BLOCK + tid; i < Q.n; i += gsize * BLOCK) __stcg(Q.dist + i, inf);
+    }
+    return;
+  }
+  unsigned long long local_claim = 0;
+  const unsigned long long count = d_hi - d_lo;
+  if (mode == PH_M_HUB) {
+    for (;;) {
+      /* a stale chunk skips expand() and its barriers: every thread must have
+       * read this iteration's S.stop / S.total before thread 0 rewrites them */
+      __syncthreads();
+      if (tid == 0) {
+        S.claim = solo ? local_claim++ : atomicAdd(&G->work, 1ull) - d_wb;
+        S.stop = 1u;
+        if (S.claim < count) {
+          const uint4 h = __ldcg(reinterpret_cast<const uint4 *>(hub_of(P, c) + d_lo + S.claim));
+          /* h = {v, d, eb, ee}.  The row's vertex improved since the chunk was
+           * cut: a later expansion covers these edges with the smaller value */
+          if (__ldcg(Q.dist + h.x) == h.y) {
+            S.it_rb[0] = h.z;
+            S.it_du[0] = h.y;
+            S.it_off[0] = 0u;
+            S.total = h.w - h.z;
+            ++S.st_hubs;
+          } else {
+            S.total = 0u;
+            ++S.st_stale;
+          }
+          S.stop = 0u;
+        }
+      }
+      __syncthreads();
+      if (S.stop) break;
+      expand<FLT, BLOCK>(P, c, S, Q, 1u, S.total, d_base);
+    }
+    flush<BLOCK>(P, c, S);
+    return;
+  }
+  /* LIGHT / HEAVY: chunks of BLOCK entries of list d_list */
+  const bool light = mode == PH_M_LIGHT;
+  const unsigned *__restrict__ row = Q.row;
+  const unsigned *__restrict__ split = Q.split;
+  for (;;) {
+    if (tid == 0) {
+      S.claim = solo ? local_claim++ : atomicAdd(&G->work, 1ull) - d_wb;
+      S.stop = S.claim * BLOCK >= count ? 1u : 0u;
+      if (!S.stop) {
+        const unsigned long long s0 = d_lo + S.claim * BLOCK;
+        const unsigned long long s1 = min(s0 + BLOCK, d_hi) - 1ull;
+        S.pi0 = pt_lookup(P, c, d_list, s0 >> PH_PAGE_LOG2);
+        S.pi1 = ((s1 >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2))
+                    ? S.pi0
+                    : pt_lookup(P, c, d_list, s1 >> PH_PAGE_LOG2);
+        ++S.st_chunks;
+        S.st_items += s1 + 1ull - s0;
+      }
+    }
+    __syncthreads();
+    if (S.stop) break;
+    const unsigned long long s0 = d_lo + S.claim * BLOCK;
+    const unsigned k = (unsigned)min((unsigned long long)BLOCK, d_hi - s0);
+    unsigned deg = 0, rb = 0, du = 0;
+    bool stale = false, repush = false;
+    if (tid < k) {
+      const unsigned long long idx = s0 + tid;
+      const unsigned pg = ((idx >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2)) ? S.pi0 : S.pi1;
+      if (pg != 0xFFFFFFFFu) {
+        const unsigned long long e = __ldcg(entry_ptr(P, c, pg, idx));
+        const unsigned v = (unsigned)e, d = (unsigned)(e >> 32);
+        if (__ldcg(Q.dist + v) != d) {
+          stale = true; /* superseded: a later push carries the smaller value */
+        } else {
+          const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
+          if (b > d_base) { /* left in the far slot: move it to its own bucket */
+            stage<BLOCK>(S, v, d, route(b, d_base));
+            repush = true;
+          } else {
+            const unsigned r0 = __ldg(row + v), r1 = __ldg(row + v + 1);
+            const unsigned nl = split ? __ldg(split + v) : (r1 - r0);
+            if (light) {
+              rb = r0;
+              deg = nl;
+              if (nl < r1 - r0) stage<BLOCK>(S, v, d, PH_LSETTLED);
+            } else {
+              rb = r0 + nl;
+              deg = r1 - rb;
+            }
+            if (deg > P.hub_threshold) { /* cut into chunks for the whole group */
+              const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
+              const unsigned hb = atomicAdd(&G->hub_count, nch);
+              if (hb + nch > P.hub_cap) {
+                raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
+              } else {
+                PhHub *hp = hub_of(P, c) + hb;
+                for (unsigned j = 0; j < nch; ++j)
+                  __stcg(reinterpret_cast<uint4 *>(hp + j),
+                         make_uint4(v, d, rb + j * P.hub_chunk,
+                                    rb + min(deg, (j + 1u) * P.hub_chunk)));
+              }
+              deg = 0;
+            }
+            du = d;
+          }
+        }
+      }
+    }
+    S.it_rb[tid] = rb;
+    S.it_du[tid] = du;
+    const unsigned nstale = __syncthreads_count(stale);
+    const unsigned nrepush = __syncthreads_count(repush);
+    if (tid == 0) {
+      S.st_stale += nstale;
+      S.st_repush += nrepush;
+      if (!light) S.st_heavy += k - nstale - nrepush;
+    }
+    unsigned tot;
+    const unsigned off = block_exscan<BLOCK>(S, deg, tot);
+    S.it_off[tid] = off;
+    __syncthreads();
+    /* the entry step staged up to BLOCK pushes: keep a round's worth of room */
+    if (S.pcnt > PSmem<BLOCK>::SB - PSmem<BLOCK>::U * BLOCK - BLOCK) flush<BLOCK>(P, c, S);
+    expand<FLT, BLOCK>(P, c, S, Q, k, tot, d_base);
+  }
+  flush<BLOCK>(P, c, S);
+}
+
+/* ------------------------------------------------------------------------ */
+/* The leader's decision (warp 0 of the last CTA to reach the barrier): what
+ * the group runs next.  Replaces the assign manager's bucket advance and
+ * termination logic (wl.h:851-1527) with a read of the list tails. */
+template <bool FLT, int BLOCK>
+__device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
+  const unsigned lane = threadIdx.x & 31u;
+  PhGroup *G = grp_of(P, c);
+  const unsigned prev_mode = S.D.mode, prev_q = S.D.q;
+  unsigned mode = PH_M_EXIT, q = prev_q, list = 0, base = ld_rlx32(&G->base);
+  unsigned long long lo = 0, hi = 0;
+  bool decide = false, next_query = false;
+  if (ld_rlx32(&P.g->err) != 0u) {
+    mode = PH_M_EXIT;
+  } else if (prev_mode == PH_M_START) {
+    next_query = true;
+  } else if (prev_mode == PH_M_INIT) {
+    /* distances are INF: set the source and push it (the first bucket) */
+    if (lane == 0) {
+      const PhQuery &Q = P.qs[prev_q];
+      const unsigned src = (P.single_src != 0xFFFFFFFFu && prev_q == 0u) ? P.single_src : Q.src;
+      st_rlx32(Q.dist + src, 0u);
+      unsigned long long b, cvp = ~0ull;
+      unsigned pg[PH_RES_PAGES], cpi = 0;
+      if (list_reserve(P, c, PH_LNEXT, 1u, &b, pg, &cvp, &cpi))
+        st_rlx64(entry_ptr(P, c, pg[0], b), (unsigned long long)src);
+      st_rlx32(&G->base, 0u);
+      __threadfence();
+    }
+    __syncwarp();
+    base = 0u;
+    decide = true;
+  } else if (prev_mode != PH_M_HUB && ld_rlx32(&G->hub_count) != 0u) {
+    mode = PH_M_HUB;
+    lo = 0;
+    hi = min(ld_rlx32(&G->hub_count), P.hub_cap);
+  } else {
+    if (prev_mode == PH_M_HUB && lane == 0) st_rlx32(&G->hub_count, 0u);
+    decide = true;
+  }
+  if (decide) {
+    const unsigned long long tn = ld_rlx64(&G->tails[PH_LNEXT].tail);
+    const unsigned long long hn = ld_rlx64(&G->head[PH_LNEXT]);
+    const unsigned long long ts = ld_rlx64(&G->tails[PH_LSETTLED].tail);
+    const unsigned long long hs = ld_rlx64(&G->head[PH_LSETTLED]);
+    if (tn > hn) {
+      mode = PH_M_LIGHT;
+      list = PH_LNEXT;
+      lo = hn;
+      hi = tn;
+    } else if (ts > hs) {
+      mode = PH_M_HEAVY;
+      list = PH_LSETTLED;
+      lo = hs;
+      hi = ts;
+    } else {
+      /* advance: the nearest non-empty slot above the base */
+      const unsigned offa = lane + 1u, offb = lane + 33u;
+      const unsigned sa = (base + offa) & (PH_NSLOT - 1u);
+      const unsigned sb = (base + offb) & (PH_NSLOT - 1u);
+      const unsigned long long ta = ld_rlx64(&G->tails[sa].tail), ha = ld_rlx64(&G->head[sa]);
+      unsigned long long tb = 0, hb = 0;
+      if (offb < PH_NSLOT) {
+        tb = ld_rlx64(&G->tails[sb].tail);
+        hb = ld_rlx64(&G->head[sb]);
+      }
+      const unsigned ma = __ballot_sync(0xFFFFFFFFu, ta > ha);
+      const unsigned mb = __ballot_sync(0xFFFFFFFFu, offb < PH_NSLOT && tb > hb);
+      if (ma | mb) {
+        const unsigned off = ma ? (unsigned)__ffs(ma) : 32u + (unsigned)__ffs(mb);
+        const unsigned sl = (base + off) & (PH_NSLOT - 1u);
+        mode = PH_M_LIGHT;
+        list = sl;
+        base += off;
+        lo = ld_rlx64(&G->head[sl]);
+        hi = ld_rlx64(&G->tails[sl].tail);
+        if (lane == 0) st_rlx32(&G->base, base);
+      } else {
+        next_query = true;
+      }
+    }
+    if ((mode == PH_M_LIGHT || mode == PH_M_HEAVY) && lane == 0) st_rlx64(&G->head[list], hi);
+  }
+  if (next_query) {
+    unsigned qi = 0;
+    if (lane == 0) qi = atomicAdd(&P.g->next_q, 1u);
+    qi = __shfl_sync(0xFFFFFFFFu, qi, 0);
+    if (qi < P.nq) {
+      mode = PH_M_INIT;
+      q = P.order ? P.order[qi] : qi;
+      base = 0u;
+      /* a new query: lists start on a page boundary (the pool restarts) */
+      for (unsigned L = lane; L < PH_NLIST; L += 32u) {
+        const unsigned long long t = ld_rlx64(&G->tails[L].tail);
+        const unsigned long long al = (t + PH_PAGE - 1ull) & ~(unsigned long long)(PH_PAGE - 1u);
+        st_rlx64(&G->tails[L].tail, al);
+        st_rlx64(&G->head[L], al);
+      }
+      if (lane == 0) {
+        st_rlx32(&G->page_next, 0u);
+        st_rlx32(&G->hub_count, 0u);
+        st_rlx32(&G->q, q);
+        st_rlx32(&G->base, 0u);
+      }
+    } else {
+      mode = PH_M_EXIT;
+    }
+  }
+  const unsigned long long wb = ld_rlx64(&G->work);
+  __syncwarp();
+  if (lane == 0) {
+    S.D.mode = mode;
+    S.D.q = q;
+    S.D.list = list;
+    S.D.base = base;
+    S.D.lo = lo;
+    S.D.hi = hi;
+    S.D.work_base = wb;
+    S.D.catchall = 0u;
+  }
+}
+
+/* frontiers small enough for the leader alone */
+template <int BLOCK>
+__device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK> &S) {
+  const unsigned mode = S.D.mode;
+  if (mode == PH_M_LIGHT || mode == PH_M_HEAVY) return S.D.hi - S.D.lo <= P.solo_max;
+  if (mode == PH_M_HUB) return S.D.hi - S.D.lo <= 1ull;
+  if (mode == PH_M_INIT) return P.qs[S.D.q].n <= 64u * BLOCK;
+  return false;
+}
+
+/* ------------------------------------------------------------------------ */
+template <bool FLT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constant__ PhParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PSmem<BLOCK> &S = *reinterpret_cast<PSmem<BLOCK> *>(smem_raw);
+  const unsigned tid = threadIdx.x;
+  Ctx c;
+  c.gi = blockIdx.x / P.gsize;
+  c.rank = blockIdx.x % P.gsize;
+  c.deadline = gtimer() + P.timeout_ns;
+  c.edges = 0;
+  PhGroup *G = grp_of(P, c);
+  unsigned long long cy_work = 0, cy_wait = 0, cy_lead = 0, nphase = 0;
+  const long long cy0 = clock64();
+  if (tid == 0) {
+    S.gen = ld_acq32(&G->gen);
+    S.pcnt = 0u;
+    S.D.mode = PH_M_START;
+    S.D.q = 0u;
+    S.st_items = S.st_stale = S.st_heavy = S.st_repush = S.st_pushes = S.st_chunks = 0;
+    S.st_hubs = S.st_solo = 0;
+  }
+  if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
+  __syncthreads();
+  for (;;) {
+    const long long t0 = clock64();
+    run_phase<FLT, BLOCK>(P, c, S, false);
+    const long long t1 = clock64();
+    cy_work += (unsigned long long)(t1 - t0);
+    /* group barrier: the last CTA in becomes the leader */
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const unsigned old = atomicAdd(&G->arrive, 1u);
+      S.leader = (old == P.gsize - 1u) ? 1u : 0u;
+      if (S.leader) {
+        st_rlx32(&G->arrive, 0u);
+        __threadfence();
+      }
+    }
+    __syncthreads();
+    if (S.leader) {
+      for (;;) {
+        if (tid < 32) leader_step<FLT, BLOCK>(P, c, S);
+        __syncthreads();
+        ++nphase;
+        if (!solo_ok<BLOCK>(P, S)) break;
+        if (tid == 0) ++S.st_solo;
+        run_phase<FLT, BLOCK>(P, c, S, true);
+        __syncthreads();
+        if (tid == 0) __threadfence();
+        __syncthreads();
+      }
+      if (tid == 0) {
+        G->desc[(S.gen + 1u) & 1u] = S.D;
+        __threadfence();
+        st_rel32(&G->gen, S.gen + 1u);
+      }
+      cy_lead += (unsigned long long)(clock64() - t1);
+    } else {
+      if (tid == 0) {
+        Waiter w{c.deadline, 0};
+        bool ok = true;
+        while (ld_acq32(&G->gen) == S.gen) {
+          if (!w.spin(P.g, W_BARRIER, 256)) {
+            ok = false;
+            break;
+          }
+        }
+        if (ok) {
+          const PhDesc *dp = &G->desc[(S.gen + 1u) & 1u];
+          S.D.mode = ld_rlx32(&dp->mode);
+          S.D.q = ld_rlx32(&dp->q);
+          S.D.list = ld_rlx32(&dp->list);
+          S.D.base = ld_rlx32(&dp->base);
+          S.D.lo = ld_rlx64(&dp->lo);
+          S.D.hi = ld_rlx64(&dp->hi);
+          S.D.work_base = ld_rlx64(&dp->work_base);
+        } else {
+          S.D.mode = PH_M_EXIT;
+        }
+      }
+      cy_wait += (unsigned long long)(clock64() - t1);
+    }
+    if (tid == 0) ++S.gen;
+    __syncthreads();
+    if (S.D.mode == PH_M_EXIT) break;
+  }
+  /* statistics */
+  PhGlobal *g = P.g;
+  unsigned long long s_edges = c.edges;
+  for (int o = 16; o > 0; o >>= 1) s_edges += __shfl_down_sync(0xFFFFFFFFu, s_edges, o);
+  if ((tid & 31u) == 0u && s_edges) atomicAdd(&g->st_edges, s_edges);
+  if (tid == 0) {
+    atomicAdd(&g->st_items, S.st_items);
+    atomicAdd(&g->st_stale, S.st_stale);
+    atomicAdd(&g->st_heavy, S.st_heavy);
+    atomicAdd(&g->st_repush, S.st_repush);
+    atomicAdd(&g->st_pushes, S.st_pushes);
+    atomicAdd(&g->st_chunks, S.st_chunks);
+    atomicAdd(&g->st_hub, S.st_hubs);
+    atomicAdd(&g->st_solo, S.st_solo);
+    atomicAdd(&g->st_phases, nphase);
+    atomicAdd(&g->st_cyc[0], cy_work);
+    atomicAdd(&g->st_cyc[1], cy_wait);
+    atomicAdd(&g->st_cyc[2], cy_lead);
+    atomicAdd(&g->st_cyc[3], (unsigned long long)(clock64() - cy0));
+  }
+}
+
+template <bool FLT, int BLOCK, int MINB>
+static cudaError_t prep_one(int *max_blocks_per_sm) {
+  const size_t smem = sizeof(PSmem<BLOCK>);
+  cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
+                                                       phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
+}
+
+template <bool FLT, int BLOCK, int MINB>
+static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
+  /* cooperative launch: every CTA of a group waits at the group barrier, so
+   * all of them must be resident; the Ex form keeps it graph-capturable */
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.groups * P.gsize);
+  cfg.blockDim = dim3(BLOCK);
+  cfg.dynamicSmemBytes = sizeof(PSmem<BLOCK>);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB>, P);
+}
+
+}  // namespace adds_phase
+
+/* Kernel variants: (threads per CTA, CTAs per SM the registers are sized
+ * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1, 3: 512 x 1 (128
+ * registers per thread), 4: 256 x 2 (128 registers). */
+#define PH_VARIANTS(X) X(0, 256, 4) X(1, 512, 2) X(2, 1024, 1) X(3, 512, 1) X(4, 256, 2)
+
+int adds_phase_variant_block(int variant) {
+#define X(i, b, m) if (variant == i) return b;
+  PH_VARIANTS(X)
+#undef X
+  return 0;
+}
+
+cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm) {
+  using namespace adds_phase;
+#define X(i, b, m) \
+  if (variant == i) return flt ? prep_one<true, b, m>(max_blocks_per_sm) : prep_one<false, b, m>(max_blocks_per_sm);
+  PH_VARIANTS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st) {
+  using namespace adds_phase;
+#define X(i, b, m) \
+  if (variant == i) return P.is_float ? launch_one<true, b, m>(P, st) : launch_one<false, b, m>(P, st);
+  PH_VARIANTS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+/* ======================================================================== */
+/* host side                                                                  */
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+
+static unsigned ph_log2_ceil(unsigned long long x) {
+  unsigned l = 0;
+  while ((1ull << l) < x) ++l;
+  return l;
+}
+
+void ph_engine_free(PhEngine &E) {
+  void *ptrs[] = {E.grp, E.g, E.qs, E.order, E.pool, E.pt, E.hub};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (E.g_host) cudaFreeHost(E.g_host);
+  E = PhEngine();
+}
+
+/* Full reset (first use, or after a device error left a barrier or a list
+ * half way): group state and page tables back to their initial values. */
+int ph_engine_reset(PhEngine &E, cudaStream_t st) {
+  if (cudaMemsetAsync(E.grp, 0, (size_t)E.groups * sizeof(PhGroup), st) != cudaSuccess ||
+      cudaMemsetAsync(E.pt, 0xFF, ((size_t)E.groups * PH_NLIST << E.ptn_log2) * 8, st) !=
+          cudaSuccess ||
+      cudaMemsetAsync(E.g, 0, sizeof(PhGlobal), st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return -5; /* ADDS_ERR_CUDA */
+  return 0;
+}
+
+int ph_engine_upload(PhEngine &E, cudaStream_t st) {
+  if (cudaMemcpyAsync(E.qs, E.qs_host.data(), E.qs_host.size() * sizeof(PhQuery),
+                      cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return -5;
+  return 0;
+}
+
+static int ph_blocks_per_sm(bool flt, int variant, int *bps) {
+  return adds_phase_prepare(flt, variant, bps) == cudaSuccess ? 0 : -5;
+}
+
+/* Sizes the per-group pools for the largest query (x grow) and allocates. */
+int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery> &qv,
+                    const PhKnobs &k, unsigned grow, cudaStream_t st) {
+  ph_engine_free(E);
+  E.device = device;
+  E.flt = flt;
+  E.nq = (unsigned)qv.size();
+  E.variant = (unsigned)k.variant;
+  E.block = (unsigned)adds_phase_variant_block(k.variant);
+  int bps = 0;
+  if (E.block == 0 || ph_blocks_per_sm(flt, k.variant, &bps) || bps < 1)
+    return -9; /* ADDS_ERR_UNSUPPORTED */
+  if (cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return -5;
+  const int cps = (k.ctas_per_sm > 0 && k.ctas_per_sm < bps) ? k.ctas_per_sm : bps;
+  const unsigned nctas = (unsigned)(cps * E.num_sms);
+  if (E.nq == 1) {
+    E.gsize = nctas;
+    E.groups = 1;
+  } else {
+    unsigned gs = k.group_ctas > 0 ? (unsigned)k.group_ctas
+                                   : std::max(1u, nctas / std::min(E.nq, 64u));
+    gs = std::min(gs, nctas);
+    E.gsize = gs;
+    E.groups = std::min(nctas / gs, E.nq);
+  }
+  double need = 0;
+  unsigned long long mmax = 0;
+  for (const PhQuery &q : qv) {
+    need = std::max(need, 3.0 * q.n + q.m / 8.0);
+    mmax = std::max(mmax, q.m);
+    E.max_n = std::max(E.max_n, q.n);
+  }
+  const unsigned long long pages = (unsigned long long)(need * grow / PH_PAGE) + 2ull * PH_NLIST + 8ull;
+  if (pages > 0x3FFFFFFFull) return -4; /* ADDS_ERR_OOM */
+  E.pages_per_group = (unsigned)pages;
+  E.ptn_log2 = ph_log2_ceil(pages + 2ull);
+  E.hub_cap = (unsigned)std::min<unsigned long long>(
+      0x7FFFFFFFull, 2ull * (mmax / std::max(64u, k.hub_chunk)) + 4096ull);
+  E.qs_host = qv;
+#define PH_ALLOC(ptr, bytes_)                               \
+  do {                                                      \
+    size_t _b = (bytes_);                                   \
+    if (cudaMalloc((void **)&(ptr), _b) != cudaSuccess) {   \
+      cudaGetLastError();                                   \
+      ph_engine_free(E);                                    \
+      return -4;                                            \
+    }                                                       \
+    E.bytes += _b;                                          \
+  } while (0)
+  PH_ALLOC(E.grp, (size_t)E.groups * sizeof(PhGroup));
+  PH_ALLOC(E.g, sizeof(PhGlobal));
+  PH_ALLOC(E.qs, (size_t)E.nq * sizeof(PhQuery));
+  PH_ALLOC(E.order, (size_t)E.nq * 4);
+  PH_ALLOC(E.pool, (size_t)E.groups * E.pages_per_group * PH_PAGE * 8);
+  PH_ALLOC(E.pt, ((size_t)E.groups * PH_NLIST << E.ptn_log2) * 8);
+  PH_ALLOC(E.hub, (size_t)E.groups * E.hub_cap * sizeof(PhHub));
+#undef PH_ALLOC
+  if (cudaMallocHost((void **)&E.g_host, sizeof(PhGlobal)) != cudaSuccess) {
+    cudaGetLastError();
+    ph_engine_free(E);
+    return -4;
+  }
+  memset(E.g_host, 0, sizeof(PhGlobal));
+  /* largest queries first: the last group to finish is not stuck with a big one */
+  std::vector<unsigned> order(E.nq);
+  for (unsigned i = 0; i < E.nq; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](unsigned a, unsigned b) {
+    return qv[a].m + qv[a].n > qv[b].m + qv[b].n;
+  });
+  if (cudaMemcpyAsync(E.order, order.data(), (size_t)E.nq * 4, cudaMemcpyHostToDevice, st) !=
+      cudaSuccess)
+    return -5;
+  int rc = ph_engine_upload(E, st);
+  if (rc) return rc;
+  return ph_engine_reset(E, st);
+}
+
+int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P) {
+  memset(P, 0, sizeof *P);
+  P->qs = E.qs;
+  P->order = E.order;
+  P->nq = E.nq;
+  P->groups = E.groups;
+  P->gsize = E.gsize;
+  P->grp = E.grp;
+  P->g = E.g;
+  P->pool = E.pool;
+  P->pages_per_group = E.pages_per_group;
+  P->pt = E.pt;
+  P->ptn_log2 = E.ptn_log2;
+  P->hub = E.hub;
+  P->hub_cap = E.hub_cap;
+  P->hub_threshold = std::max(64u, k.hub_threshold);
+  P->hub_chunk = std::max(64u, std::min(k.hub_chunk, P->hub_threshold));
+  P->solo_max = k.solo_max;
+  P->is_float = E.flt ? 1u : 0u;
+  P->single_src = single_src;
+  P->timeout_ns = k.timeout_ns;
+  return 0;
+}
+
+/* One launch: statistics cleared, the persistent kernel, the control block
+ * copied back (it carries the error word).  Graph-capturable. */
+int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent_t k0,
+                      cudaEvent_t k1) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return -5;
+  const unsigned fl = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+  if (cudaMemsetAsync(E.g, 0, sizeof(PhGlobal), st) != cudaSuccess) return -5;
+  if (k0 && cudaEventRecordWithFlags(k0, st, fl) != cudaSuccess) return -5;
+  if (adds_phase_launch(P, (int)E.variant, st) != cudaSuccess) return -5;
+  if (k1 && cudaEventRecordWithFlags(k1, st, fl) != cudaSuccess) return -5;
+  if (cudaMemcpyAsync(E.g_host, E.g, sizeof(PhGlobal), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return -5;
+  return 0;
+}
+
+/* device error word -> ABI code (after the stream has been synchronised) */
+int ph_engine_status(const PhEngine &E, char *msg, size_t msg_len) {
+  const unsigned err = E.g_host->err;
+  if (err && msg) snprintf(msg, msg_len, "device error %u at wait site %u", err, E.g_host->err_where);
+  switch (err) {
+    case 0: return 0;
+    case PH_ERR_OVERFLOW: return -7;     /* ADDS_ERR_WL_OVERFLOW    */
+    case PH_ERR_HUB_OVERFLOW: return -7;
+    case PH_ERR_MAPPING: return -5;      /* engine fault: ADDS_ERR_CUDA */
+    default: return -6;                  /* ADDS_ERR_DEVICE_TIMEOUT */
+  }
+}

@@ -1,0 +1,191 @@
+/*
+ * phase_internal.h — device data layout of the bulk-synchronous bucket
+ * engine (phase.cu).
+ *
+ * The reference worklist (ads_int/wl.h:133-190) keeps 32 circular distance
+ * buckets as virtual ranges of a paged HBM pool and lets workers pop and push
+ * asynchronously under three manager warps (wl.h:488-1527).  This engine keeps
+ * the bucket ring and the paged pool but runs the buckets in phases: a group
+ * of CTAs expands one frontier (a range of one list), meets at a group
+ * barrier, and the last CTA to arrive (the leader) decides the next frontier.
+ * Inside a phase nothing waits for anything but a page mapping, so the edge
+ * stream runs at full width; between phases the leader's decision is one read
+ * of a few list tails.
+ *
+ * Lists are append-only for the life of the engine: a list is a monotone
+ * 64-bit index space [head, tail) whose 4096-entry virtual pages map to pool
+ * pages through a per-list ring of page-table cells tagged with the virtual
+ * page number.  Pool pages are handed out by a per-group bump counter that is
+ * reset when the group starts a query (the lists of the previous query are
+ * empty by then), so nothing is ever freed or recycled inside a solve.
+ */
+#ifndef ADDS_PHASE_INTERNAL_H_
+#define ADDS_PHASE_INTERNAL_H_
+
+#include <stdint.h>
+
+#define PH_NSLOT 64                /* bucket ring (the reference has 32 bags)   */
+#define PH_LNEXT PH_NSLOT          /* list: current bucket's next frontier     */
+#define PH_LSETTLED (PH_NSLOT + 1) /* list: settled vertices with heavy edges  */
+#define PH_NLIST (PH_NSLOT + 2)
+#define PH_PAGE_LOG2 12
+#define PH_PAGE (1u << PH_PAGE_LOG2) /* entries per pool page (8 B each)      */
+
+/* phase modes */
+#define PH_M_INIT 0u   /* fill the query's distances with INF                 */
+#define PH_M_LIGHT 1u  /* expand light edges of a list range                  */
+#define PH_M_HEAVY 2u  /* expand heavy edges of settled vertices              */
+#define PH_M_HUB 3u    /* expand split-row chunks                             */
+#define PH_M_EXIT 4u   /* no more queries for this group                      */
+
+/* device error codes (first one wins) */
+#define PH_ERR_TIMEOUT 1u
+#define PH_ERR_OVERFLOW 2u
+#define PH_ERR_HUB_OVERFLOW 3u
+#define PH_ERR_MAPPING 4u
+
+/* Read-only per-query descriptor. */
+struct PhQuery {
+  const unsigned *row;   /* n+1 row offsets                                   */
+  const uint2 *edges;    /* m x {dst, weight bits}; rows weight-sorted when
+                            split != NULL                                     */
+  const unsigned *split; /* light edges (w < delta) at the start of each row  */
+  unsigned *dist;        /* n distance words                                  */
+  unsigned n;
+  unsigned src;
+  float scale;           /* float graphs: key = floor(d * scale)              */
+  unsigned shift;        /* bucket = key >> shift                             */
+  unsigned long long m;
+};
+
+/* One split-row chunk: edges [eb, ee) of vertex v expanded with distance d. */
+struct __align__(16) PhHub {
+  unsigned v, d, eb, ee;
+};
+
+/* What every CTA of a group needs for one phase (written by the leader before
+ * it releases the barrier; double-buffered by barrier generation). */
+struct __align__(64) PhDesc {
+  unsigned mode;
+  unsigned q;                  /* query index                                */
+  unsigned list;               /* list the frontier is read from             */
+  unsigned base;               /* absolute bucket being settled              */
+  unsigned long long lo, hi;   /* entry range of the list (hub: record range) */
+  unsigned long long work_base; /* claim counter value at phase start        */
+  unsigned catchall;           /* the range may hold entries of later buckets */
+  unsigned pad[5];
+};
+
+/* Per-group state.  `arrive` and `gen` sit in lines of their own; the list
+ * tails are hit by reservations from every CTA of the group, each in its own
+ * 128-byte line. */
+struct __align__(128) PhTail {
+  unsigned long long tail;
+  unsigned long long pad[15];
+};
+
+struct __align__(128) PhGroup {
+  unsigned arrive;
+  unsigned pad0[31];
+  unsigned gen;
+  unsigned pad1[31];
+  unsigned long long work;     /* chunk claim counter (monotone)             */
+  unsigned long long pad2[15];
+  unsigned hub_count;          /* split-row chunks appended this phase       */
+  unsigned pad3[31];
+  unsigned page_next;          /* bump allocator: next free page (relative)  */
+  unsigned pad4[31];
+  PhDesc desc[2];
+  /* leader-only control state */
+  unsigned q;                  /* current query                              */
+  unsigned base;               /* absolute base bucket                       */
+  unsigned mode;               /* mode of the phase that just ran            */
+  unsigned pad5[29];
+  unsigned long long head[PH_NLIST];
+  PhTail tails[PH_NLIST];
+};
+
+/* Engine-wide control and statistics. */
+struct __align__(128) PhGlobal {
+  unsigned err;
+  unsigned err_where;
+  unsigned pad0[30];
+  unsigned next_q;             /* batch: next query to hand to a group       */
+  unsigned pad1[31];
+  unsigned long long st_items, st_stale, st_edges, st_pushes, st_chunks, st_hub,
+      st_phases, st_solo, st_heavy, st_repush, st_pages;
+  unsigned long long st_cyc[4]; /* SM cycles summed over CTAs: work, barrier
+                                   wait, leader, total                        */
+  unsigned long long st_pad[1];
+};
+
+/* Kernel parameters (by value). */
+struct PhParams {
+  const PhQuery *qs;
+  const unsigned *order;       /* query order (largest first); NULL = 0..nq-1 */
+  unsigned nq;
+  unsigned groups;             /* CTA groups; gridDim.x = groups * gsize      */
+  unsigned gsize;              /* CTAs per group                             */
+  PhGroup *grp;                /* [groups]                                   */
+  PhGlobal *g;
+  unsigned long long *pool;    /* groups * pages_per_group * PH_PAGE entries  */
+  unsigned pages_per_group;
+  unsigned long long *pt;      /* groups * PH_NLIST << ptn_log2 cells         */
+  unsigned ptn_log2;
+  PhHub *hub;                  /* groups * hub_cap records                    */
+  unsigned hub_cap;
+  unsigned hub_threshold;      /* rows with more expanded edges are split     */
+  unsigned hub_chunk;          /* edges per split chunk                       */
+  unsigned solo_max;           /* frontiers up to this size run on the leader */
+  unsigned is_float;
+  unsigned single_src;         /* overrides query 0's source when != ~0       */
+  unsigned long long timeout_ns;
+};
+
+#ifdef __cplusplus
+#include <cuda_runtime.h>
+#include <vector>
+
+/* Host-side handle of one engine instance (phase.cu). */
+struct PhEngine {
+  int device = -1;
+  bool flt = false;
+  unsigned nq = 0, groups = 0, gsize = 0, block = 0, variant = 0;
+  unsigned pages_per_group = 0, ptn_log2 = 0, hub_cap = 0, max_n = 0;
+  PhGroup *grp = nullptr;
+  PhGlobal *g = nullptr;
+  PhQuery *qs = nullptr;
+  unsigned *order = nullptr;
+  unsigned long long *pool = nullptr, *pt = nullptr;
+  PhHub *hub = nullptr;
+  PhGlobal *g_host = nullptr; /* pinned copy of the statistics and error word */
+  std::vector<PhQuery> qs_host;
+  size_t bytes = 0;
+  int num_sms = 0;
+};
+
+/* knobs of one launch */
+struct PhKnobs {
+  int variant;        /* kernel variant (threads x CTAs per SM), phase.cu      */
+  int ctas_per_sm;    /* <= 0: as many as fit                                 */
+  int group_ctas;     /* CTAs per group (batches); <= 0: automatic            */
+  unsigned hub_threshold, hub_chunk, solo_max;
+  unsigned long long timeout_ns;
+};
+
+/* phase.cu host API (C++ linkage) */
+int adds_phase_variant_block(int variant);
+cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm);
+cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st);
+int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery> &qv,
+                    const PhKnobs &k, unsigned grow, cudaStream_t st);
+void ph_engine_free(PhEngine &E);
+int ph_engine_reset(PhEngine &E, cudaStream_t st);
+int ph_engine_upload(PhEngine &E, cudaStream_t st);
+int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P);
+int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent_t k0,
+                      cudaEvent_t k1);
+int ph_engine_status(const PhEngine &E, char *msg, size_t msg_len);
+#endif
+
+#endif /* ADDS_PHASE_INTERNAL_H_ */

@@ -237,8 +237,8 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
     srcs = pick_sources(g, wl, csr_row)
     tuned, tune_ms = None, None
     if not args.no_tune:
-        tuned, tune_ms = g.tune(srcs[:2])
-    opts = A.default_opts(timeout_ms=60000)
+        tuned, tune_ms = g.tune(srcs[:2], A.default_opts(engine=args.engine))
+    opts = A.default_opts(timeout_ms=60000, engine=args.engine)
     # per-source reached vertices / edges (outside the timed region)
     mr, nr = {}, {}
     for s in srcs:
@@ -320,10 +320,14 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
             "device_sum_of_solves_s": st["ms"] / 1e3,
             "work_gteps_last": None, "edges_scanned_last": work_edges,
             "items_last": st["items_popped"], "stale_last": st["items_stale"],
-            "pushes_last": st["pushes"], "ctas": st["ctas"],
-            "tuned": ({k: getattr(tuned, k) for k in ("delta_shift", "window", "batch_max",
-                                                        "hub_threshold", "ctas_per_sm",
-                                                        "strict_order")} if tuned else None),
+            "pushes_last": st["pushes"], "ctas": st["ctas"], "engine": st["engine"],
+            "phases_last": st["phases"], "solo_phases_last": st["solo_phases"],
+            "chunks_last": st["batches"], "phase_cycles_last": st["phase_cycles"],
+            "tuned": ({k: getattr(tuned, k) for k in ("engine", "delta_shift", "block_threads",
+                                                        "ctas_per_sm", "solo_max",
+                                                        "hub_threshold", "light_heavy", "window",
+                                                        "batch_max", "strict_order")}
+                      if tuned else None),
             "tune_ms_per_solve": tune_ms,
         },
     }
@@ -577,6 +581,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--engine", type=int, default=0, help="0 auto, 1 async, 2 phase")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

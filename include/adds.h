@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define ADDS_ABI_VERSION 1
+#define ADDS_ABI_VERSION 2
 
 typedef enum { ADDS_I32 = 0, ADDS_F32 = 1 } adds_wtype;
 
@@ -73,10 +73,23 @@ typedef struct adds_opts {
   int32_t light_heavy;   /* 1: relax heavy edges (w >= delta) once per settled
                             vertex from a weight-sorted row copy; 0: off;
                             <0 = auto (on)                                     */
-  int32_t block_threads; /* threads per persistent CTA: 128, 256 or 512; 0 = auto */
-  int32_t greed;         /* a claim takes avail / (CTAs >> greed) entries; <0 = auto */
-  int32_t reserved[2];
+  int32_t block_threads; /* threads per persistent CTA: async engine 128, 256 or
+                            512; phase engine 256, 512 or 1024; 0 = auto       */
+  int32_t greed;         /* async engine: a claim takes avail / (CTAs >> greed)
+                            entries; <0 = auto                                 */
+  int32_t engine;        /* ADDS_ENGINE_*: 0 = auto (phase)                      */
+  int32_t group_ctas;    /* phase engine, batches: CTAs that solve one query
+                            together; 0 = auto                                 */
+  int32_t solo_max;      /* phase engine: frontiers of at most this many entries
+                            run on one CTA without a group barrier; <0 = auto  */
+  int32_t reserved[5];
 } adds_opts;
+
+/* Engines.  PHASE settles the buckets in bulk-synchronous phases (light
+ * edges to convergence, then heavy edges once) with the frontier spread
+ * over every CTA; ASYNC pops and pushes bucket entries asynchronously with
+ * per-bucket counters, as the reference's worklist does. */
+enum { ADDS_ENGINE_AUTO = 0, ADDS_ENGINE_ASYNC = 1, ADDS_ENGINE_PHASE = 2 };
 
 /* Per-solve statistics (reference: work_count + fd-3 record,
  * ads_int/kernel.cu:264-282). */
@@ -101,7 +114,11 @@ typedef struct adds_stats {
   int32_t delta_shift;      /* bucket shift at the end of the solve            */
   int32_t retries;          /* worklist regrowths needed                       */
   int32_t ctas;             /* persistent CTAs launched                        */
-  int32_t reserved[5];
+  int32_t engine;           /* ADDS_ENGINE_ASYNC or ADDS_ENGINE_PHASE          */
+  int32_t reserved[4];
+  uint64_t phases;          /* phase engine: phases decided (solo included)    */
+  uint64_t solo_phases;     /* phase engine: phases run by one CTA             */
+  uint64_t repushes;        /* phase engine: far-slot entries moved on         */
 } adds_stats;
 
 typedef struct adds_graph_info_t {
@@ -250,9 +267,13 @@ int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_start,
                       uint32_t *dist, void *stream);
 
 /* ---- autotuner ---------------------------------------------------------- */
-/* Times candidate (delta, window, CTAs/SM, batch, hub threshold) settings on
- * the sample sources and stores the fastest in the graph (used whenever a
- * later call passes "auto" knobs).  best may be NULL. */
+/* Times candidate settings on the sample sources and stores the fastest in
+ * the graph (used whenever a later call passes "auto" knobs): delta, then for
+ * the phase engine the kernel variant (threads x CTAs per SM), the solo
+ * threshold, the split-row threshold and the light/heavy split; for the async
+ * engine window, batch, hub threshold, block, greed, CTAs/SM, order and local
+ * chaining.  best may be NULL; if not, best->engine selects the engine to
+ * tune on input (0 = auto) and *best receives the winner. */
 int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns,
               adds_opts *best, double *best_ms);
 

@@ -9,6 +9,9 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 OPTS = dict(timeout_ms=10000)
+ASYNC, PHASE = 1, 2
+# phase-engine kernel variants: (threads per CTA, CTAs per SM)
+VARIANTS = [(512, 2), (256, 4), (1024, 1), (512, 1), (256, 2)]
 
 
 def _check(g, src, **kw):
@@ -23,27 +26,61 @@ def _check(g, src, **kw):
     return st
 
 
-def test_rmat16_int_max_degree_source():
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
+def test_rmat16_int_max_degree_source(engine):
     g = G.rmat(16, 16, seed=1)
-    st = _check(g, G.max_degree_vertex(g))
-    assert st["items_popped"] > 0
+    st = _check(g, G.max_degree_vertex(g), engine=engine)
+    assert st["items_popped"] > 0 and st["engine"] == engine
 
 
-def test_grid_float_with_shortcuts():
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
+def test_grid_float_with_shortcuts(engine):
     g = G.grid(256, 256, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=3)
-    _check(g, 128 * 256 + 128)
+    _check(g, 128 * 256 + 128, engine=engine)
 
 
-def test_erdos_renyi_int():
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
+def test_erdos_renyi_int(engine):
     g = G.erdos_renyi(20000, 8, seed=11)
-    _check(g, 5)
+    _check(g, 5, engine=engine)
 
 
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
 @pytest.mark.parametrize("shift", [0, 4, 9, 14, 20])
 @pytest.mark.parametrize("lh", [0, 1])
-def test_any_delta_gives_same_distances(shift, lh):
+def test_any_delta_gives_same_distances(engine, shift, lh):
     g = G.rmat(13, 16, seed=2)
-    _check(g, G.max_degree_vertex(g), delta_shift=shift, light_heavy=lh)
+    _check(g, G.max_degree_vertex(g), delta_shift=shift, light_heavy=lh, engine=engine)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("solo", [0, 64, 100000])
+@pytest.mark.parametrize("lh", [0, 1])
+def test_phase_schedules_int_rmat(variant, solo, lh):
+    """Kernel variants, solo-CTA thresholds (0: never, 100000: whole solve on
+    one CTA) and split rows (hub threshold 64 edges) all give the oracle's
+    distances; shift 1 overflows the bucket ring into the far slot."""
+    g = G.rmat(12, 16, seed=5, w_hi=10000)
+    for shift in (1, 6, 9, 12):
+        _check(g, 3, engine=PHASE, delta_shift=shift, light_heavy=lh, solo_max=solo,
+               block_threads=variant[0], ctas_per_sm=variant[1], hub_threshold=64)
+
+
+@pytest.mark.parametrize("variant", VARIANTS[:3])
+@pytest.mark.parametrize("lh", [0, 1])
+def test_phase_schedules_float_grid(variant, lh):
+    g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=8)
+    for shift in (6, 12, 16, 20):
+        _check(g, 40 * 96 + 48, engine=PHASE, delta_shift=shift, light_heavy=lh,
+               block_threads=variant[0], ctas_per_sm=variant[1], solo_max=256)
+
+
+def test_phase_float_grid_large_keys():
+    """A high-diameter float grid with a narrow bucket (many slots, far-slot
+    re-pushes) and zero-weight edges mixed in."""
+    g = G.grid(200, 150, 0.02, 8, wtype=G.F32, w_lo=0.0, w_hi=3.0, seed=12)
+    for shift in (8, 14):
+        _check(g, 0, engine=PHASE, delta_shift=shift, solo_max=128)
 
 
 @pytest.mark.parametrize("window", [1, 2, 4])
@@ -53,8 +90,8 @@ def test_any_delta_gives_same_distances(shift, lh):
 def test_schedules_int_rmat(window, lh, local, block):
     g = G.rmat(12, 16, seed=5, w_hi=10000)
     for shift in (6, 9, 12):
-        _check(g, 3, delta_shift=shift, window=window, light_heavy=lh, local_max=local,
-               block_threads=block, hub_threshold=256)
+        _check(g, 3, engine=ASYNC, delta_shift=shift, window=window, light_heavy=lh,
+               local_max=local, block_threads=block, hub_threshold=256)
 
 
 @pytest.mark.parametrize("window", [1, 2])
@@ -63,23 +100,25 @@ def test_schedules_int_rmat(window, lh, local, block):
 def test_schedules_float_grid(window, lh, block):
     g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=8)
     for shift in (12, 16, 20):
-        _check(g, 40 * 96 + 48, delta_shift=shift, window=window, light_heavy=lh,
-               block_threads=block)
+        _check(g, 40 * 96 + 48, engine=ASYNC, delta_shift=shift, window=window,
+               light_heavy=lh, block_threads=block)
 
 
 def test_non_strict_order():
     g = G.rmat(12, 16, seed=6, w_hi=10000)
     for lh in (0, 1):
-        _check(g, 1, strict_order=0, light_heavy=lh, delta_shift=8)
+        _check(g, 1, engine=ASYNC, strict_order=0, light_heavy=lh, delta_shift=8)
 
 
-def test_batch_mixed_graphs_replayed_twice():
+@pytest.mark.parametrize("engine,group", [(ASYNC, 0), (PHASE, 0), (PHASE, 1), (PHASE, 7),
+                                          (PHASE, 1000)])
+def test_batch_mixed_graphs_replayed_twice(engine, group):
     gs = [G.erdos_renyi(3000 + 997 * i, 8, seed=100 + i) for i in range(5)]
     r = G.rmat(12, 16, seed=9)
     graphs = [A.Graph.from_csr(g) for g in gs] + [A.Graph.from_csr(r)]
     qg = graphs + [graphs[-1]] * 3
     srcs = [0, 1, 2, 3, 4, G.max_degree_vertex(r), 1, 2, 3]
-    b = A.Batch(qg, srcs, A.default_opts(**OPTS))
+    b = A.Batch(qg, srcs, A.default_opts(**OPTS, engine=engine, group_ctas=group))
     csrs = gs + [r] * 4
     for _ in range(2):  # second run replays the captured CUDA graph
         st = b.run()
