@@ -151,6 +151,21 @@ class Graph:
         check(lib().adds_graph_reached(self._h, C.byref(r), C.byref(e)), "adds_graph_reached")
         return r.value, e.value
 
+    def trace(self, cap: int) -> None:
+        """Records up to cap phases of each later solve (0 turns it off)."""
+        check(lib().adds_graph_trace(self._h, cap), "adds_graph_trace")
+
+    def trace_read(self, cap: int = 1 << 16):
+        """The last solve's phase records as a numpy structured array
+        (t_ns, count, mode, base) and the number the solve produced."""
+        import numpy as np
+        dt = np.dtype([("t_ns", "<u8"), ("count", "<u4"), ("mode", "<u2"), ("base", "<u2")])
+        buf = np.zeros(cap, dtype=dt)
+        n = C.c_uint64()
+        check(lib().adds_graph_trace_read(self._h, buf.ctypes.data, cap, C.byref(n)),
+              "adds_graph_trace_read")
+        return buf[: min(cap, n.value)], n.value
+
     def tune(self, srcs, base: Opts | None = None):
         arr = (C.c_uint32 * len(srcs))(*srcs)
         best = Opts()

@@ -162,6 +162,9 @@ SIGNATURES = [
     ("adds_batch_backward", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("adds_sssp_backward", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.POINTER(Opts)]),
+    ("adds_graph_trace", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("adds_graph_trace_read", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32,
+                                        C.POINTER(C.c_uint64)]),
     ("adds_tune", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Opts),
                             C.POINTER(C.c_double)]),
     ("adds_write_dist_text", C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_int]),

@@ -21,6 +21,10 @@
 #define ADDS_PAGE (1u << ADDS_PAGE_LOG2) /* entries per pool page (8 B each)   */
 #define ADDS_HUB_RING_LOG2 16      /* split-row chunk ring capacity            */
 #define ADDS_INF_I32_BITS 0x7FFFFFFFu
+/* Graph edge arrays are allocated this many entries past m: the phase
+ * engine copies row segments rounded out to 16-byte boundaries, so a copy
+ * may read one entry past the last row (never relaxed). */
+#define ADDS_EDGE_PAD 2u
 #define ADDS_INF_F32_BITSV 0x7F7FFFFFu
 
 /* device error codes written to GlobalCtl::err (first one wins) */

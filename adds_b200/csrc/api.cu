@@ -270,11 +270,12 @@ struct Knobs {
   unsigned long long timeout_ns;
 };
 
-/* phase-engine kernel variant for (threads per CTA, CTAs per SM) */
+/* phase-engine kernel variant for threads per CTA (the CTAs per SM follow
+ * from its shared memory) */
 static int phase_variant(int block, int cps) {
-  if (block == 256) return cps == 2 ? 4 : 0;
   if (block == 1024) return 2;
-  return cps == 1 ? 3 : 1;
+  if (block == 512) return cps == 1 ? 4 : 1;
+  return cps == 2 ? 3 : 0;
 }
 
 static PhKnobs phase_knobs(const Knobs &k) {
@@ -283,7 +284,7 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.ctas_per_sm = 0;
   p.group_ctas = k.group_ctas;
   p.hub_threshold = (unsigned)std::max(64, k.hub_threshold);
-  p.hub_chunk = 4096u;
+  p.hub_chunk = 1024u;
   p.solo_max = (unsigned)std::max(0, k.solo_max);
   p.timeout_ns = k.timeout_ns;
   return p;
@@ -398,6 +399,7 @@ struct adds_graph {
   size_t bytes = 0;
   Engine eng;
   PhEngine peng;       /* phase engine (allocated on first use)            */
+  unsigned trace_cap = 0; /* phase trace records requested (0 = off)       */
   PhParams last_pp;
   int last_engine = 0; /* engine of the solves in flight                   */
   unsigned grow = 1;
@@ -553,7 +555,7 @@ static int graph_upload(adds_graph *g, const unsigned *row_host_u32, const uint3
                         const void *w) {
   const size_t m = g->m;
   CK(cudaMalloc(&g->row, ((size_t)g->n + 1) * 4));
-  CK(cudaMalloc(&g->edges, (m ? m : 1) * sizeof(uint2)));
+  CK(cudaMalloc(&g->edges, (m + ADDS_EDGE_PAD) * sizeof(uint2)));
   g->bytes = ((size_t)g->n + 1) * 4 + m * sizeof(uint2);
   CK(cudaMemcpyAsync(g->row, row_host_u32, ((size_t)g->n + 1) * 4, cudaMemcpyHostToDevice, g->stream));
   /* stream dst/w through device staging buffers in chunks */
@@ -834,12 +836,12 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   k->greed = o->greed >= 0 ? o->greed : (t->greed >= 0 ? t->greed : 4);
   k->engine = o->engine > 0 ? o->engine : (t->engine > 0 ? t->engine : ADDS_ENGINE_PHASE);
   if (k->engine != ADDS_ENGINE_ASYNC) k->engine = ADDS_ENGINE_PHASE;
-  const int hub_def = k->engine == ADDS_ENGINE_PHASE ? 4096 : 16384;
+  const int hub_def = k->engine == ADDS_ENGINE_PHASE ? 512 : 16384;
   k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : hub_def);
   k->hub_chunk = 4096;
   if (k->engine == ADDS_ENGINE_PHASE) {
-    const int pb = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 512);
-    const int pc = o->ctas_per_sm > 0 ? o->ctas_per_sm : (t->ctas_per_sm > 0 ? t->ctas_per_sm : 2);
+    const int pb = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 256);
+    const int pc = o->ctas_per_sm > 0 ? o->ctas_per_sm : (t->ctas_per_sm > 0 ? t->ctas_per_sm : 4);
     k->variant = phase_variant(pb, pc);
   } else {
     k->variant = 0;
@@ -885,7 +887,8 @@ static int graph_sorted(adds_graph *g) {
   if (g->sorted_valid) return ADDS_OK;
   const size_t m = g->m;
   if (!g->sedges) {
-    CK(cudaMalloc(&g->sedges, (m ? m : 1) * sizeof(uint2)));
+    CK(cudaMalloc(&g->sedges, (m + ADDS_EDGE_PAD) * sizeof(uint2)));
+    CK(cudaMemsetAsync(g->sedges + m, 0, ADDS_EDGE_PAD * sizeof(uint2), g->stream));
     g->bytes += m * sizeof(uint2);
   }
   if (m == 0) {
@@ -1002,7 +1005,7 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.shift = (unsigned)shift;
   q.m = g->m;
   PhEngine &E = g->peng;
-  if (E.nq == 1 && E.variant == (unsigned)k.variant) {
+  if (E.nq == 1 && E.variant == (unsigned)k.variant && ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
     PhQuery &h = E.qs_host[0];
     if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)
       return ADDS_OK;
@@ -1011,11 +1014,35 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   }
   std::vector<PhQuery> qv(1, q);
   rc = ph_engine_alloc(E, g->device, g->wt == ADDS_F32, qv, phase_knobs(k), g->grow, g->stream);
+  if (!rc && g->trace_cap) rc = ph_engine_trace(E, g->trace_cap);
   if (rc) {
     snprintf(g_last_err, sizeof g_last_err, "phase engine allocation failed (%d)", rc);
     ph_engine_free(E);
   }
   return rc;
+}
+
+extern "C" int adds_graph_trace(adds_graph *g, uint32_t cap) {
+  if (!g || cap > (1u << 24)) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(g->stream));
+  g->trace_cap = cap;
+  if (g->peng.nq) return ph_engine_trace(g->peng, cap);
+  return ADDS_OK;
+}
+
+extern "C" int adds_graph_trace_read(adds_graph *g, adds_phase_trace *out, uint32_t cap,
+                                     uint64_t *written) {
+  if (!g) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(g->stream));
+  const uint64_t w = g->peng.nq ? g->peng.g_host->st_trace : 0;
+  if (written) *written = w;
+  const uint64_t n = std::min<uint64_t>(std::min<uint64_t>(w, g->peng.trace_cap), cap);
+  if (out && n) CK(cudaMemcpy(out, g->peng.trace, n * sizeof(PhTrace), cudaMemcpyDeviceToHost));
+  return ADDS_OK;
 }
 
 static int phase_status(const PhEngine &E) { return ph_engine_status(E, g_last_err, sizeof g_last_err); }
@@ -1065,7 +1092,7 @@ static int sssp_enqueue(adds_graph *g, uint32_t src, const adds_opts *opts) {
   CK(cudaEventRecord(ev[0], st));
   if (phase) {
     PhParams P;
-    ph_engine_params(g->peng, phase_knobs(k), src, &P);
+    if (ph_engine_params(g->peng, phase_knobs(k), src, &P)) return ADDS_ERR_INVALID;
     g->last_pp = P;
     rc = ph_engine_enqueue(g->peng, P, st, ev[1], ev[2]);
     if (rc) return cuda_fail(cudaGetLastError(), "phase engine launch");
@@ -1638,7 +1665,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   try_field(&adds_opts::delta_shift, shifts);
   if (k.engine == ADDS_ENGINE_PHASE) {
     /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
-    const int combos[5][2] = {{512, 2}, {256, 4}, {1024, 1}, {512, 1}, {256, 2}};
+    const int combos[5][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}};
     for (const auto &cb : combos) {
       adds_opts t = cur;
       t.block_threads = cb[0];
@@ -1651,7 +1678,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
       }
     }
     try_field(&adds_opts::solo_max, {0, 256, 512, 1024, 2048, 4096});
-    try_field(&adds_opts::hub_threshold, {1024, 4096, 16384});
+    try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
     try_field(&adds_opts::light_heavy, {0, 1});
     if (cur.delta_shift != s0) {
       std::vector<int> s2;

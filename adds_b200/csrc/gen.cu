@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include "../../include/adds.h"
+#include "adds_internal.h"
 
 namespace adds_gen {
 
@@ -200,7 +201,8 @@ extern "C++" int adds_gen_build(const adds_gen_spec *sp, unsigned **row_out, uin
     if (last == ~0ull) --m; /* drop the invalid-key run */
   }
   if (cudaMalloc(&row, ((size_t)n + 1) * 4) != cudaSuccess ||
-      cudaMalloc(&edges, (m ? m : 1) * sizeof(uint2)) != cudaSuccess) {
+      cudaMalloc(&edges, (m + ADDS_EDGE_PAD) * sizeof(uint2)) != cudaSuccess ||
+      cudaMemsetAsync(edges + m, 0, ADDS_EDGE_PAD * sizeof(uint2), st) != cudaSuccess) {
     rc = ADDS_ERR_OOM;
     goto done;
   }

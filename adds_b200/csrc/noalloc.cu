@@ -7,10 +7,10 @@
  * synchronises the whole device), or a latency-bound service loop where the
  * implicit synchronisation of cudaMalloc/cudaFree is not acceptable.
  * adds_sssp_noalloc serves them: the caller passes the graph and the output
- * as device arrays it already owns, and all the engine's working memory
- * (bucket page pool, page tables, bucket counters, split-row ring, control
- * block) comes from one file-scope device array of fixed size declared
- * below.  The array exists on every GPU that loads this library, from the
+ * as device arrays it already owns, and all the working memory of the phase
+ * engine (bucket page pool, page tables, list tails, split-row records,
+ * control block) comes from one file-scope device array of fixed size
+ * declared below.  The array exists on every GPU that loads this library, from the
  * moment the library's code is loaded on it until the process exits.
  *
  * Limits: n <= ADDS_NOALLOC_MAX_N vertices, m <= ADDS_NOALLOC_MAX_M edges;
@@ -30,39 +30,32 @@
 
 #include "../../include/adds.h"
 #include "adds_internal.h"
+#include "phase_internal.h"
 
-/* engine.cu */
-cudaError_t adds_engine_prepare(bool flt, int block, int *max_blocks_per_sm);
-cudaError_t adds_engine_launch_init(const EngParams &P, unsigned max_n, cudaStream_t st);
-cudaError_t adds_engine_launch_solve(const EngParams &P, int block, cudaStream_t st);
-cudaError_t adds_engine_launch_reset(unsigned long long *fq, unsigned fq_cells,
-                                     unsigned pool_pages, unsigned *hub_seq, unsigned hub_cells,
-                                     cudaStream_t st);
 void adds_set_last_error(const char *msg);
 
 namespace {
 
 /* layout of the scratch array (byte offsets) */
-constexpr unsigned kPoolPages = 1536;              /* 1536 x 4096 entries x 8 B = 48 MiB */
-constexpr unsigned kFqCells = 2048;                /* power of two >= kPoolPages        */
-constexpr unsigned kPtnLog2 = 11;                  /* page-table ring per slot           */
-constexpr unsigned kHubCells = 1u << ADDS_HUB_RING_LOG2;
-constexpr size_t kOffG = 0;                                        /* GlobalCtl  */
-constexpr size_t kOffQd = 4096;                                    /* QueryDesc  */
-constexpr size_t kOffCtl = kOffQd + 256;                           /* QueryCtl   */
-constexpr size_t kOffSum = kOffCtl + 256;                          /* weight sum */
-constexpr size_t kOffSlots = 8192;                                 /* 2*NB slots */
-constexpr size_t kOffPgen = kOffSlots + 2 * ADDS_NB * sizeof(SlotCtr);
-constexpr size_t kOffPcons = kOffPgen + kPoolPages * 4;
-constexpr size_t kOffFq = (kOffPcons + kPoolPages * 4 + 255) & ~size_t(255);
-constexpr size_t kOffHubSeq = kOffFq + kFqCells * 8;
-constexpr size_t kOffHub = (kOffHubSeq + kHubCells * 4 + 255) & ~size_t(255);
-constexpr size_t kOffPt = kOffHub + (size_t)kHubCells * sizeof(HubChunk);
-constexpr size_t kPtWords = (size_t)2 * ADDS_NB << kPtnLog2;
-constexpr size_t kOffPool = (kOffPt + kPtWords * 8 + 4095) & ~size_t(4095);
-constexpr size_t kEnd = kOffPool + (size_t)kPoolPages * ADDS_PAGE * 8;
-static_assert(sizeof(GlobalCtl) <= kOffQd, "control block does not fit");
-static_assert(sizeof(QueryDesc) <= 256 && sizeof(QueryCtl) <= 256, "descriptor does not fit");
+constexpr unsigned kVariant = 0;        /* phase kernel: 256 threads, 4 CTAs per SM   */
+constexpr unsigned kHubThreshold = 512; /* rows longer than this are split          */
+constexpr unsigned kPtnLog2 = 11;       /* page-table ring per list (>= kPages + 2) */
+constexpr unsigned kPages = 1792;       /* 1792 pages x 4096 entries x 8 B = 56 MiB */
+constexpr unsigned kHubCap = 4u * (ADDS_NOALLOC_MAX_M / kHubThreshold) + 4096u;
+constexpr size_t kOffG = 0;                                        /* PhGlobal     */
+constexpr size_t kOffGrp = 4096;                                   /* PhGroup      */
+constexpr size_t kOffQd = kOffGrp + 16384;                         /* PhQuery      */
+constexpr size_t kOffSum = kOffQd + 256;                           /* weight sum   */
+constexpr size_t kOffPt = kOffSum + 256;
+constexpr size_t kPtBytes = ((size_t)PH_NLIST << kPtnLog2) * 8;
+constexpr size_t kOffHub = (kOffPt + kPtBytes + 255) & ~size_t(255);
+constexpr size_t kOffHubSeq = kOffHub + (size_t)kHubCap * sizeof(PhHub);
+constexpr size_t kOffPool = (kOffHubSeq + (size_t)kHubCap * 4 + 4095) & ~size_t(4095);
+constexpr size_t kEnd = kOffPool + (size_t)kPages * PH_PAGE * 8;
+static_assert(sizeof(PhGlobal) <= kOffGrp, "control block does not fit");
+static_assert(sizeof(PhGroup) <= kOffQd - kOffGrp, "group state does not fit");
+static_assert(sizeof(PhQuery) <= 256, "descriptor does not fit");
+static_assert((1u << kPtnLog2) >= kPages + 2u, "page-table ring smaller than the pool");
 static_assert(kEnd <= ADDS_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the array");
 
 }  // namespace
@@ -74,13 +67,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[ADDS_NOALLOC_SC
 
 namespace {
 
-__global__ void na_setup(GlobalCtl *g, QueryDesc *qd, QueryDesc desc, unsigned pool_pages,
-                         double *wsum) {
-  /* clear-to-zero state was memset by the host; set the rest */
-  g->fq_tail = pool_pages;
-  *qd = desc;
-  *wsum = 0.0;
-}
+__global__ void na_setup(PhQuery *qd, PhQuery desc) { *qd = desc; }
 
 /* mean of evenly spaced weights (the delta heuristic needs the scale) */
 __global__ void na_sample(const uint2 *edges, unsigned long long m, int is_float, unsigned ns,
@@ -122,7 +109,6 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   DevState &D = g_dev[dev];
   cudaStream_t st = (cudaStream_t)stream;
   const bool flt = wt == ADDS_F32;
-  const int block = 256;
 #define NA_CK(x)                                  \
   do {                                            \
     cudaError_t _e = (x);                         \
@@ -140,8 +126,8 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
     void *p = nullptr;
     NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     int bps_i = 0, bps_f = 0, sms = 0;
-    NA_CK(adds_engine_prepare(false, block, &bps_i));
-    NA_CK(adds_engine_prepare(true, block, &bps_f));
+    NA_CK(adds_phase_prepare(false, kVariant, &bps_i));
+    NA_CK(adds_phase_prepare(true, kVariant, &bps_f));
     NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bps = bps_i < bps_f ? bps_i : bps_f;
     if (bps < 1) return ADDS_ERR_UNSUPPORTED;
@@ -149,17 +135,13 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
     D.base = (unsigned char *)p;
   }
   unsigned char *B = D.base;
-  GlobalCtl *g = (GlobalCtl *)(B + kOffG);
-  QueryDesc *qd = (QueryDesc *)(B + kOffQd);
-  QueryCtl *ctl = (QueryCtl *)(B + kOffCtl);
+  PhGlobal *g = (PhGlobal *)(B + kOffG);
+  PhGroup *grp = (PhGroup *)(B + kOffGrp);
+  PhQuery *qd = (PhQuery *)(B + kOffQd);
   double *wsum = (double *)(B + kOffSum);
-  SlotCtr *slots = (SlotCtr *)(B + kOffSlots);
-  unsigned *pgen = (unsigned *)(B + kOffPgen);
-  unsigned *pcons = (unsigned *)(B + kOffPcons);
-  unsigned long long *fq = (unsigned long long *)(B + kOffFq);
-  unsigned *hub_seq = (unsigned *)(B + kOffHubSeq);
-  HubChunk *hub = (HubChunk *)(B + kOffHub);
   unsigned long long *pt = (unsigned long long *)(B + kOffPt);
+  PhHub *hub = (PhHub *)(B + kOffHub);
+  unsigned *hub_seq = (unsigned *)(B + kOffHubSeq);
   unsigned long long *pool = (unsigned long long *)(B + kOffPool);
 
   /* the delta heuristic of the allocating path: bucket width from the mean
@@ -182,16 +164,14 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   while (shift < 31 && (double)(1u << (shift + 1)) <= dk * 1.41421356) ++shift;
 
   /* clear the state that must start at zero (the array keeps the previous
-   * call's contents) */
-  NA_CK(cudaMemsetAsync(pool, 0, (size_t)kPoolPages * ADDS_PAGE * 8, st));
-  NA_CK(cudaMemsetAsync(g, 0, sizeof(GlobalCtl), st));
-  NA_CK(cudaMemsetAsync(ctl, 0, sizeof(QueryCtl), st));
-  NA_CK(cudaMemsetAsync(slots, 0, 2 * ADDS_NB * sizeof(SlotCtr), st));
-  NA_CK(cudaMemsetAsync(pgen, 0, kPoolPages * 4, st));
-  NA_CK(cudaMemsetAsync(pcons, 0, kPoolPages * 4, st));
-  NA_CK(cudaMemsetAsync(pt, 0xFF, kPtWords * 8, st));
-  NA_CK(adds_engine_launch_reset(fq, kFqCells, kPoolPages, hub_seq, kHubCells, st));
-  QueryDesc desc;
+   * call's contents): group barrier and lists, statistics and error word,
+   * page-table tags, split-row record sequence words.  Pool pages are always
+   * written before they are read. */
+  NA_CK(cudaMemsetAsync(g, 0, sizeof(PhGlobal), st));
+  NA_CK(cudaMemsetAsync(grp, 0, sizeof(PhGroup), st));
+  NA_CK(cudaMemsetAsync(pt, 0xFF, kPtBytes, st));
+  NA_CK(cudaMemsetAsync(hub_seq, 0, (size_t)kHubCap * 4, st));
+  PhQuery desc;
   memset(&desc, 0, sizeof desc);
   desc.row = row_start;
   desc.edges = (const uint2 *)edges;
@@ -200,53 +180,43 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   desc.n = n;
   desc.src = src;
   desc.scale = scale;
-  desc.ptn_log2 = kPtnLog2;
-  desc.pt = pt;
-  desc.slots = slots;
-  desc.ctl = ctl;
-  desc.shift0 = (unsigned)shift;
-  desc.graph_id = 0;
-  na_setup<<<1, 1, 0, st>>>(g, qd, desc, kPoolPages, wsum);
+  desc.shift = (unsigned)shift;
+  desc.m = m;
+  na_setup<<<1, 1, 0, st>>>(qd, desc);
   NA_CK(cudaGetLastError());
 
-  EngParams P;
+  PhParams P;
   memset(&P, 0, sizeof P);
   P.qs = qd;
+  P.order = nullptr;
   P.nq = 1;
-  P.nctas = (unsigned)D.ctas;
+  P.groups = 1;
+  P.gsize = (unsigned)D.ctas;
+  P.grp = grp;
   P.g = g;
   P.pool = pool;
-  P.pgen = pgen;
-  P.pcons = pcons;
-  P.fq = fq;
-  P.fq_mask = kFqCells - 1u;
-  P.pool_pages = kPoolPages;
+  P.pages_per_group = kPages;
+  P.pt = pt;
+  P.ptn_log2 = kPtnLog2;
   P.hub = hub;
   P.hub_seq = hub_seq;
-  P.timeout_ns = 20000ull * 1000000ull;
-  P.alloc_wait_ns = 200ull * 1000000ull;
-  P.window = 2;
-  P.batch_max = block;
-  P.hub_threshold = 16384;
-  P.hub_chunk = 4096;
-  P.strict_order = 1;
-  P.adapt = 0;
+  P.hub_cap = kHubCap;
+  P.hub_threshold = kHubThreshold;
+  P.hub_chunk = kHubThreshold;
+  P.solo_max = 1024;
   P.is_float = flt ? 1u : 0u;
   P.single_src = 0xFFFFFFFFu;
-  P.local_max = block;
-  P.local_max_hungry = block / 8;
-  P.block = block;
-  P.greed = 4;
-  NA_CK(adds_engine_launch_init(P, n, st));
-  NA_CK(adds_engine_launch_solve(P, block, st));
+  P.timeout_ns = 20000ull * 1000000ull;
+  NA_CK(adds_phase_launch(P, kVariant, st));
   unsigned err[2] = {0, 0};
   NA_CK(cudaMemcpyAsync(err, &g->err, 8, cudaMemcpyDeviceToHost, st));
   NA_CK(cudaStreamSynchronize(st));
 #undef NA_CK
-  if (err[0] == ADDS_DEV_OK) return ADDS_OK;
+  if (err[0] == 0u) return ADDS_OK;
   char msg[120];
   snprintf(msg, sizeof msg, "device error %u at wait site %u", err[0], err[1]);
   adds_set_last_error(msg);
-  return (err[0] == ADDS_DEV_OVERFLOW || err[0] == ADDS_DEV_HUB_OVERFLOW) ? ADDS_ERR_WL_OVERFLOW
-                                                                          : ADDS_ERR_DEVICE_TIMEOUT;
+  if (err[0] == PH_ERR_OVERFLOW || err[0] == PH_ERR_HUB_OVERFLOW) return ADDS_ERR_WL_OVERFLOW;
+  if (err[0] == PH_ERR_MAPPING) return ADDS_ERR_CUDA;
+  return ADDS_ERR_DEVICE_TIMEOUT;
 }

@@ -63,6 +63,10 @@ __device__ __forceinline__ void st_rlx32(unsigned *p, unsigned v) {
 __device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+/* fire-and-forget atomic minimum (no result, so the thread does not wait) */
+__device__ __forceinline__ void red_min(unsigned *p, unsigned v) {
+  asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 /* L2 policy for the edge stream: each edge is read about once per solve, so
  * its lines go first and the distance array keeps its place in L2. */
 __device__ __forceinline__ unsigned long long evict_first_policy() {
@@ -78,7 +82,7 @@ __device__ __forceinline__ uint2 ld_edge(const uint2 *p, unsigned long long pol)
   return r;
 }
 
-enum : unsigned { W_BARRIER = 1, W_PT = 2, W_ALLOC = 3, W_MAPPING = 4, W_HUB = 5 };
+enum : unsigned { W_BARRIER = 1, W_PT = 2, W_ALLOC = 3, W_MAPPING = 4, W_HUB = 5, W_COPY = 6 };
 
 __device__ __forceinline__ void raise_err(PhGlobal *g, unsigned code, unsigned where) {
   if (atomicCAS(&g->err, 0u, code) == 0u) st_rlx32(&g->err_where, where);
@@ -119,17 +123,25 @@ __device__ __forceinline__ unsigned route(unsigned b, unsigned base) {
 
 /* ------------------------------------------------------------------------ */
 /* shared memory of one CTA                                                   */
-#define PH_RES_PAGES 4u /* pages one list reservation may touch (flush size) */
+#define PH_RES_PAGES 6u /* pages one list reservation may touch (flush size) */
+/* split-row chunk records one CTA takes at a time */
+#define PH_HUB_PER_CLAIM(BLOCK) ((BLOCK) / 16u)
 
-template <int BLOCK>
+template <int BLOCK, int UU>
 struct PSmem {
-  static constexpr int U = 4;                     /* edges per thread per round */
-  static constexpr int SB = 2 * BLOCK * U + BLOCK; /* staged pushes             */
+  static constexpr int U = UU;      /* edges per thread in flight                     */
+  static constexpr int SEGI = 2;    /* iterations of U edges between flush checks     */
+  static constexpr int FLUSH_AT = 4 * BLOCK; /* flush once more than this is staged  */
+  /* staged pushes: FLUSH_AT, plus one per entry of a chunk, plus one per edge of
+   * a segment -- a segment can never overflow the buffer */
+  static constexpr int SB = FLUSH_AT + BLOCK + SEGI * U * BLOCK;
   static_assert(SB <= (int)((PH_RES_PAGES - 1u) * PH_PAGE + 1u),
                 "a flush must fit in PH_RES_PAGES pages of one list");
-  unsigned it_rb[BLOCK];                          /* first edge of each item    */
-  unsigned it_du[BLOCK];                          /* distance of each item      */
-  unsigned it_off[BLOCK];                         /* exclusive scan of degrees  */
+  /* the items of the chunk being expanded: row segments [rb, re) */
+  unsigned it_rb[BLOCK];
+  unsigned it_du[BLOCK];      /* distance the item is expanded with              */
+  unsigned it_off[BLOCK + 1]; /* exclusive scan of the segment lengths           */
+  unsigned ck_k, ck_E;        /* items and edges of the chunk                    */
   unsigned pb_v[SB];
   unsigned pb_d[SB];
   unsigned short pb_rank[SB];
@@ -168,6 +180,9 @@ __device__ __forceinline__ unsigned long long *entry_ptr(const PhParams &P, cons
 }
 __device__ __forceinline__ PhHub *hub_of(const PhParams &P, const Ctx &c) {
   return P.hub + (unsigned long long)c.gi * P.hub_cap;
+}
+__device__ __forceinline__ unsigned *hub_seq_of(const PhParams &P, const Ctx &c) {
+  return P.hub_seq + (unsigned long long)c.gi * P.hub_cap;
 }
 
 /* Page of virtual page vp of list L; waits for the reservation that owns the
@@ -242,8 +257,9 @@ __device__ __forceinline__ unsigned pt_lookup(const PhParams &P, const Ctx &c, u
 
 /* ------------------------------------------------------------------------ */
 /* staging and flushing of pushes                                             */
-template <int BLOCK>
-__device__ __forceinline__ void stage(PSmem<BLOCK> &S, unsigned v, unsigned d, unsigned L) {
+
+template <int BLOCK, int UU>
+__device__ __forceinline__ void stage(PSmem<BLOCK, UU> &S, unsigned v, unsigned d, unsigned L) {
   const unsigned mask = __activemask();
   const unsigned lane = threadIdx.x & 31u;
   const unsigned leader = __ffs(mask) - 1u;
@@ -259,15 +275,26 @@ __device__ __forceinline__ void stage(PSmem<BLOCK> &S, unsigned v, unsigned d, u
  * entry stores.  Nothing else: the phase barrier publishes them.  Replaces the
  * per-warp reservation + st.cg + __threadfence + write_done update of
  * push_work (wl.h:1902-1928).  Call with every thread, after a barrier. */
-template <int BLOCK>
-__device__ void flush(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
+template <int BLOCK, int UU>
+__device__ void flush(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   const unsigned tid = threadIdx.x;
   const unsigned cnt = S.pcnt;
   if (cnt == 0u) return;
   if (tid < PH_NLIST) S.hist[tid] = 0u;
   __syncthreads();
-  for (unsigned i = tid; i < cnt; i += BLOCK)
-    S.pb_rank[i] = (unsigned short)atomicAdd(&S.hist[S.pb_l[i]], 1u);
+  /* ranks within each list: one shared atomic per distinct list per warp */
+  const unsigned lane = tid & 31u;
+  for (unsigned i0 = tid - lane; i0 < cnt; i0 += BLOCK) {
+    const unsigned i = i0 + lane;
+    const bool in = i < cnt;
+    const unsigned L = in ? S.pb_l[i] : 0xFFu;
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, L);
+    const unsigned first = __ffs(grp) - 1u;
+    unsigned b = 0;
+    if (in && lane == first) b = atomicAdd(&S.hist[L], (unsigned)__popc(grp));
+    b = __shfl_sync(0xFFFFFFFFu, b, first);
+    if (in) S.pb_rank[i] = (unsigned short)(b + __popc(grp & ((1u << lane) - 1u)));
+  }
   __syncthreads();
   if (tid < PH_NLIST) {
     const unsigned h = S.hist[tid];
@@ -295,8 +322,8 @@ __device__ void flush(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
 }
 
 /* block-wide exclusive scan of one value per thread */
-template <int BLOCK>
-__device__ __forceinline__ unsigned block_exscan(PSmem<BLOCK> &S, unsigned x, unsigned &total) {
+template <int BLOCK, int UU>
+__device__ __forceinline__ unsigned block_exscan(PSmem<BLOCK, UU> &S, unsigned x, unsigned &total) {
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   unsigned incl = x;
 #pragma unroll
@@ -323,18 +350,223 @@ __device__ __forceinline__ unsigned block_exscan(PSmem<BLOCK> &S, unsigned x, un
 }
 
 /* ------------------------------------------------------------------------ */
-/* Edge-balanced expansion of the k items staged in S.it_* (E edges in all):
- * relax, atomicMin, stage the winners.  Each thread takes every BLOCK-th edge
- * of a round of BLOCK*U, so loads of consecutive threads are consecutive in
- * memory; the next round's edge loads are issued before this round's
- * distance gathers and atomics, so the edge stream stays in flight. */
-template <bool FLT, int BLOCK>
-__device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, const PhQuery &Q, unsigned k,
-                       unsigned E, unsigned base) {
-  constexpr int U = PSmem<BLOCK>::U;
-  constexpr unsigned R = BLOCK * U;
-  constexpr unsigned FLUSH_AT = PSmem<BLOCK>::SB - R - BLOCK;
+/* Chunks.  A chunk is up to BLOCK frontier entries (or a few split-row
+ * records); each becomes an item, a row segment [rb, re) of the CSR to
+ * expand with distance du.  The CTA scans the segment lengths, then every
+ * thread walks its share of the chunk's edges with no barrier until the
+ * chunk is done.                                                             */
+
+/* Claims and prepares the next chunk.  Returns false when the phase has no
+ * more chunks.  Every thread calls it. */
+template <bool FLT, int BLOCK, int UU>
+__device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo,
+                              unsigned long long &local_claim, unsigned long long &pend) {
   const unsigned tid = threadIdx.x;
+  const unsigned mode = S.D.mode;
+  PhGroup *G = grp_of(P, c);
+  const PhQuery &Q = P.qs[S.D.q];
+  const unsigned long long d_lo = S.D.lo, d_hi = S.D.hi, d_wb = S.D.work_base;
+  const unsigned d_base = S.D.base, d_list = S.D.list;
+  /* entries per claim: the leader spreads a medium frontier over every CTA */
+  const unsigned per = solo ? (unsigned)BLOCK : S.D.per;
+  __syncthreads(); /* everyone has read the previous claim's S.stop */
+  if (tid == 0) {
+    if (solo) {
+      S.claim = local_claim++;
+    } else {
+      /* the next claim is taken one chunk ahead, so its latency overlaps this
+       * chunk's work; claims past the end are simply not used */
+      const unsigned long long cl = pend != ~0ull ? pend : atomicAdd(&G->work, 1ull);
+      pend = atomicAdd(&G->work, 1ull);
+      S.claim = cl - d_wb;
+    }
+    S.stop = S.claim * per >= d_hi - d_lo ? 1u : 0u;
+    if (!S.stop) {
+      const unsigned long long s0 = d_lo + S.claim * per;
+      const unsigned long long s1 = min(s0 + per, d_hi) - 1ull;
+      const unsigned long long v0 = s0 >> PH_PAGE_LOG2, v1 = s1 >> PH_PAGE_LOG2;
+      S.pi0 = S.ptc_vp[d_list] == v0 ? S.ptc_pi[d_list] : pt_lookup(P, c, d_list, v0);
+      S.pi1 = v1 == v0 ? S.pi0 : pt_lookup(P, c, d_list, v1);
+      S.ptc_vp[d_list] = v1;
+      S.ptc_pi[d_list] = S.pi1;
+      ++S.st_chunks;
+      S.st_items += s1 + 1ull - s0;
+    }
+  }
+  __syncthreads();
+  if (S.stop) return false;
+  const unsigned long long s0 = d_lo + S.claim * per;
+  const unsigned k = (unsigned)min((unsigned long long)per, d_hi - s0);
+  unsigned rb = 0, re = 0, du = 0;
+  bool stale = false, repush = false;
+  if (tid < k) {
+    {
+      const unsigned long long idx = s0 + tid;
+      const unsigned pg = ((idx >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2)) ? S.pi0 : S.pi1;
+      if (pg != 0xFFFFFFFFu) {
+        const unsigned long long e = __ldcg(entry_ptr(P, c, pg, idx));
+        const unsigned v = (unsigned)e, d = (unsigned)(e >> 32);
+        if (__ldcg(Q.dist + v) != d) {
+          stale = true; /* superseded: a later push carries the smaller value */
+        } else {
+          const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
+          if (b > d_base) { /* left in the far slot: move it to its own bucket */
+            stage<BLOCK, UU>(S, v, d, route(b, d_base));
+            repush = true;
+          } else {
+            const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
+            const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
+            if (mode == PH_M_LIGHT) {
+              rb = r0;
+              re = r0 + nl;
+              if (nl < r1 - r0) stage<BLOCK, UU>(S, v, d, PH_LSETTLED);
+            } else {
+              rb = r0 + nl;
+              re = r1;
+            }
+            if (re - rb > P.hub_threshold) { /* cut into chunks for the whole group */
+              const unsigned deg = re - rb;
+              const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
+              const unsigned hb = atomicAdd(&G->hub_count, nch);
+              if (hb + nch > P.hub_cap) {
+                raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
+              } else {
+                PhHub *hp = hub_of(P, c) + hb;
+                unsigned *sq = hub_seq_of(P, c) + hb;
+                for (unsigned j = 0; j < nch; ++j)
+                  __stcg(reinterpret_cast<uint4 *>(hp + j),
+                         make_uint4(v, d, rb + j * P.hub_chunk,
+                                    rb + min(deg, (j + 1u) * P.hub_chunk)));
+                __threadfence(); /* the records before their sequence words */
+                const unsigned ep = S.D.epoch;
+                for (unsigned j = 0; j < nch; ++j) st_rlx32(sq + j, ep);
+              }
+              re = rb;
+            }
+            du = d;
+          }
+        }
+      }
+    }
+  }
+  S.it_rb[tid] = rb;
+  S.it_du[tid] = du;
+  const unsigned nstale = __syncthreads_count(stale);
+  const unsigned nrepush = __syncthreads_count(repush);
+  if (tid == 0) {
+    S.st_stale += nstale;
+    S.st_repush += nrepush;
+    if (mode == PH_M_HEAVY) S.st_heavy += k - nstale - nrepush;
+  }
+  unsigned tot;
+  const unsigned off = block_exscan<BLOCK, UU>(S, re - rb, tot);
+  S.it_off[tid] = off;
+  if (tid == 0) {
+    S.it_off[BLOCK] = tot;
+    S.ck_k = k;
+    S.ck_E = tot;
+  }
+  __syncthreads();
+  return true;
+}
+
+/* Claims the next split-row records of this phase and prepares them as the
+ * chunk.  Records are appended by CTAs that are still expanding frontier
+ * chunks (the producers); a claim beyond the records appended so far waits
+ * (bounded) until they are there or every producer has finished.  Returns
+ * false when no record is left.  Every thread calls it. */
+template <bool FLT, int BLOCK, int UU>
+__device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
+  constexpr unsigned K = PH_HUB_PER_CLAIM(BLOCK);
+  const unsigned tid = threadIdx.x;
+  PhGroup *G = grp_of(P, c);
+  const PhQuery &Q = P.qs[S.D.q];
+  const unsigned epoch = S.D.epoch;
+  __syncthreads(); /* everyone has read the previous claim's S.stop */
+  if (tid == 0) {
+    const unsigned r = atomicAdd(&G->hub_claim, K);
+    unsigned n = 0;
+    Waiter w{c.deadline, 0};
+    for (;;) {
+      const unsigned hc = ld_acq32(&G->hub_count);
+      if (hc >= r + K) {
+        n = K;
+        break;
+      }
+      if (ld_acq32(&G->producers) == 0u) { /* no record can still appear */
+        const unsigned hf = min(ld_acq32(&G->hub_count), P.hub_cap);
+        n = hf > r ? min(K, hf - r) : 0u;
+        break;
+      }
+      if (!w.spin(P.g, W_HUB, 128)) break;
+    }
+    n = r < P.hub_cap ? min(n, P.hub_cap - r) : 0u; /* past the store: overflow */
+    S.claim = r;
+    S.pi0 = n;
+    S.stop = n == 0u ? 1u : 0u;
+  }
+  __syncthreads();
+  if (S.stop) return false;
+  const unsigned r = (unsigned)S.claim, k = S.pi0;
+  unsigned rb = 0, re = 0, du = 0;
+  bool stale = false;
+  if (tid < k) {
+    /* the record's reservation was counted before it was written */
+    const unsigned *sq = hub_seq_of(P, c) + r + tid;
+    Waiter w{c.deadline, 0};
+    bool ok = true;
+    while (ld_acq32(sq) != epoch) {
+      if (!w.spin(P.g, W_HUB, 64)) {
+        ok = false;
+        break;
+      }
+    }
+    if (ok) {
+      const uint4 h = __ldcg(reinterpret_cast<const uint4 *>(hub_of(P, c) + r + tid));
+      /* h = {v, d, eb, ee}.  The row's vertex improved since the chunk was
+       * cut: a later expansion covers these edges with the smaller value */
+      if (__ldcg(Q.dist + h.x) == h.y) {
+        rb = h.z;
+        re = h.w;
+        du = h.y;
+      } else {
+        stale = true;
+      }
+    }
+  }
+  S.it_rb[tid] = rb;
+  S.it_du[tid] = du;
+  const unsigned nstale = __syncthreads_count(stale);
+  if (tid == 0) {
+    S.st_stale += nstale;
+    S.st_hubs += k - nstale;
+  }
+  unsigned tot;
+  const unsigned off = block_exscan<BLOCK, UU>(S, re - rb, tot);
+  S.it_off[tid] = off;
+  if (tid == 0) {
+    S.it_off[BLOCK] = tot;
+    S.ck_k = k;
+    S.ck_E = tot;
+  }
+  __syncthreads();
+  return true;
+}
+
+/* Relaxes the chunk's edges: in iteration i thread t takes edges
+ * i*BLOCK*U + u*BLOCK + t (u < U), so loads of neighbouring threads are
+ * neighbours in memory; it issues the loads of iteration i+1 before the
+ * distance gathers and atomicMins of iteration i.  Every SEGI iterations the
+ * CTA meets once to flush staged pushes (the staging buffer is sized so that
+ * this is the only barrier needed). */
+template <bool FLT, int BLOCK, int UU>
+__device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q,
+                       unsigned base) {
+  constexpr int U = PSmem<BLOCK, UU>::U;
+  constexpr unsigned R = BLOCK * U;
+  const unsigned tid = threadIdx.x;
+  const unsigned k = S.ck_k, E = S.ck_E;
+  const unsigned nit = (E + R - 1u) / R; /* the same for every thread */
   const uint2 *__restrict__ edges = Q.edges;
   unsigned *dist = Q.dist;
   const float scale = Q.scale;
@@ -346,7 +578,7 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, const PhQuery
   auto load_round = [&](unsigned eb) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const unsigned e = eb + u * BLOCK + tid;
+      const unsigned e = eb + u * BLOCK;
       nu[u] = 0xFFFFFFFFu;
       ne[u] = make_uint2(0u, 0u);
       if (e < E) {
@@ -360,53 +592,55 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, const PhQuery
       }
     }
   };
-  if (E) load_round(0);
+  if (nit) load_round(tid);
   unsigned nedges = 0;
-  for (unsigned eb = 0; eb < E; eb += R) {
-    uint2 ce[U];
-    unsigned nd[U];
+  for (unsigned it = 0; it < nit; ++it) {
+    unsigned dst[U], nd[U], cur[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      ce[u] = ne[u];
-      const unsigned du = nu[u];
+      dst[u] = ne[u].x;
       nd[u] = 0xFFFFFFFFu;
-      if (du != 0xFFFFFFFFu) {
-        nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(ce[u].y)))
-                    : du + ce[u].y;
+      if (nu[u] != 0xFFFFFFFFu) {
+        nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(nu[u]), __uint_as_float(ne[u].y)))
+                    : nu[u] + ne[u].y;
         ++nedges;
       }
     }
-    if (eb + R < E) load_round(eb + R);
-    unsigned cur[U];
+    if (it + 1u < nit) load_round((it + 1u) * R + tid);
 #pragma unroll
-    for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + ce[u].x) : 0u;
+    for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
+    /* an improvement on the gathered value is applied with a reduction (no
+     * return value, so no wait) and pushed at once; if a concurrent smaller
+     * value wins, the pushed entry is dropped as stale when it is popped.
+     * The reference's int kernel likewise pushes whether or not its atomicMin
+     * won (ads_int/kernel.cu:78-82). */
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (nd[u] < cur[u]) {
-        const unsigned old = atomicMin(dist + ce[u].x, nd[u]);
-        if (old > nd[u]) stage<BLOCK>(S, ce[u].x, nd[u], route(bucket_of<FLT>(nd[u], scale, shift), base));
+        red_min(dist + dst[u], nd[u]);
+        stage<BLOCK, UU>(S, dst[u], nd[u], route(bucket_of<FLT>(nd[u], scale, shift), base));
       }
     }
-    __syncthreads();
-    if (S.pcnt > FLUSH_AT) flush<BLOCK>(P, c, S);
+    if ((it % PSmem<BLOCK, UU>::SEGI) == PSmem<BLOCK, UU>::SEGI - 1u || it + 1u == nit) {
+      __syncthreads();
+      if (S.pcnt > (unsigned)PSmem<BLOCK, UU>::FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+    }
   }
   c.edges += nedges;
 }
 
 /* ------------------------------------------------------------------------ */
 /* One phase (or, solo, the whole of it on this CTA).                         */
-template <bool FLT, int BLOCK>
-__device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, bool solo) {
+template <bool FLT, int BLOCK, int UU>
+__device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo) {
+  constexpr unsigned FLUSH_AT = PSmem<BLOCK, UU>::FLUSH_AT;
   const unsigned tid = threadIdx.x;
   const unsigned mode = S.D.mode;
   if (mode == PH_M_START || mode == PH_M_EXIT) return;
-  PhGroup *G = grp_of(P, c);
   const PhQuery &Q = P.qs[S.D.q];
-  const unsigned long long d_lo = S.D.lo, d_hi = S.D.hi, d_wb = S.D.work_base;
-  const unsigned d_base = S.D.base, d_list = S.D.list;
-  const unsigned rank = solo ? 0u : c.rank;
-  const unsigned gsize = solo ? 1u : P.gsize;
   if (mode == PH_M_INIT) {
+    const unsigned rank = solo ? 0u : c.rank;
+    const unsigned gsize = solo ? 1u : P.gsize;
     const unsigned inf = P.is_float ? 0x7F7FFFFFu : 0x7FFFFFFFu;
     if ((reinterpret_cast<unsigned long long>(Q.dist) & 15ull) == 0ull) {
       uint4 *d4 = reinterpret_cast<uint4 *>(Q.dist);
@@ -419,137 +653,49 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK> &S, bool solo)
     }
     return;
   }
-  unsigned long long local_claim = 0;
-  const unsigned long long count = d_hi - d_lo;
-  if (mode == PH_M_HUB) {
-    for (;;) {
-      /* a stale chunk skips expand() and its barriers: every thread must have
-       * read this iteration's S.stop / S.total before thread 0 rewrites them */
-      __syncthreads();
+  const unsigned base = S.D.base;
+  unsigned long long local_claim = 0, pend = ~0ull;
+  /* frontier chunks first, then split-row records (a records-only phase
+   * finishes what a solo phase left) */
+  bool records = mode == PH_M_HUB;
+  for (;;) {
+    const bool have = records ? prepare_records<FLT, BLOCK, UU>(P, c, S)
+                              : prepare_chunk<FLT, BLOCK, UU>(P, c, S, solo, local_claim, pend);
+    if (!have) {
+      if (records) break;
+      /* no frontier chunk left for this CTA: it appends no more split rows,
+       * and helps expand the ones the group has appended */
+      records = true;
       if (tid == 0) {
-        S.claim = solo ? local_claim++ : atomicAdd(&G->work, 1ull) - d_wb;
-        S.stop = 1u;
-        if (S.claim < count) {
-          const uint4 h = __ldcg(reinterpret_cast<const uint4 *>(hub_of(P, c) + d_lo + S.claim));
-          /* h = {v, d, eb, ee}.  The row's vertex improved since the chunk was
-           * cut: a later expansion covers these edges with the smaller value */
-          if (__ldcg(Q.dist + h.x) == h.y) {
-            S.it_rb[0] = h.z;
-            S.it_du[0] = h.y;
-            S.it_off[0] = 0u;
-            S.total = h.w - h.z;
-            ++S.st_hubs;
-          } else {
-            S.total = 0u;
-            ++S.st_stale;
-          }
-          S.stop = 0u;
-        }
+        __threadfence();
+        PhGroup *G = grp_of(P, c);
+        atomicSub(&G->producers, 1u);
+        /* alone, with many records: leave them to the whole group */
+        S.stop = solo && ld_rlx32(&G->hub_count) - ld_rlx32(&G->hub_claim) >
+                             2u * PH_HUB_PER_CLAIM(BLOCK);
       }
       __syncthreads();
       if (S.stop) break;
-      expand<FLT, BLOCK>(P, c, S, Q, 1u, S.total, d_base);
+      continue;
     }
-    flush<BLOCK>(P, c, S);
-    return;
-  }
-  /* LIGHT / HEAVY: chunks of BLOCK entries of list d_list */
-  const bool light = mode == PH_M_LIGHT;
-  const unsigned *__restrict__ row = Q.row;
-  const unsigned *__restrict__ split = Q.split;
-  for (;;) {
-    if (tid == 0) {
-      S.claim = solo ? local_claim++ : atomicAdd(&G->work, 1ull) - d_wb;
-      S.stop = S.claim * BLOCK >= count ? 1u : 0u;
-      if (!S.stop) {
-        const unsigned long long s0 = d_lo + S.claim * BLOCK;
-        const unsigned long long s1 = min(s0 + BLOCK, d_hi) - 1ull;
-        S.pi0 = pt_lookup(P, c, d_list, s0 >> PH_PAGE_LOG2);
-        S.pi1 = ((s1 >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2))
-                    ? S.pi0
-                    : pt_lookup(P, c, d_list, s1 >> PH_PAGE_LOG2);
-        ++S.st_chunks;
-        S.st_items += s1 + 1ull - s0;
-      }
-    }
+    if (S.ck_E != 0u) expand<FLT, BLOCK, UU>(P, c, S, Q, base);
     __syncthreads();
-    if (S.stop) break;
-    const unsigned long long s0 = d_lo + S.claim * BLOCK;
-    const unsigned k = (unsigned)min((unsigned long long)BLOCK, d_hi - s0);
-    unsigned deg = 0, rb = 0, du = 0;
-    bool stale = false, repush = false;
-    if (tid < k) {
-      const unsigned long long idx = s0 + tid;
-      const unsigned pg = ((idx >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2)) ? S.pi0 : S.pi1;
-      if (pg != 0xFFFFFFFFu) {
-        const unsigned long long e = __ldcg(entry_ptr(P, c, pg, idx));
-        const unsigned v = (unsigned)e, d = (unsigned)(e >> 32);
-        if (__ldcg(Q.dist + v) != d) {
-          stale = true; /* superseded: a later push carries the smaller value */
-        } else {
-          const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
-          if (b > d_base) { /* left in the far slot: move it to its own bucket */
-            stage<BLOCK>(S, v, d, route(b, d_base));
-            repush = true;
-          } else {
-            const unsigned r0 = __ldg(row + v), r1 = __ldg(row + v + 1);
-            const unsigned nl = split ? __ldg(split + v) : (r1 - r0);
-            if (light) {
-              rb = r0;
-              deg = nl;
-              if (nl < r1 - r0) stage<BLOCK>(S, v, d, PH_LSETTLED);
-            } else {
-              rb = r0 + nl;
-              deg = r1 - rb;
-            }
-            if (deg > P.hub_threshold) { /* cut into chunks for the whole group */
-              const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
-              const unsigned hb = atomicAdd(&G->hub_count, nch);
-              if (hb + nch > P.hub_cap) {
-                raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
-              } else {
-                PhHub *hp = hub_of(P, c) + hb;
-                for (unsigned j = 0; j < nch; ++j)
-                  __stcg(reinterpret_cast<uint4 *>(hp + j),
-                         make_uint4(v, d, rb + j * P.hub_chunk,
-                                    rb + min(deg, (j + 1u) * P.hub_chunk)));
-              }
-              deg = 0;
-            }
-            du = d;
-          }
-        }
-      }
-    }
-    S.it_rb[tid] = rb;
-    S.it_du[tid] = du;
-    const unsigned nstale = __syncthreads_count(stale);
-    const unsigned nrepush = __syncthreads_count(repush);
-    if (tid == 0) {
-      S.st_stale += nstale;
-      S.st_repush += nrepush;
-      if (!light) S.st_heavy += k - nstale - nrepush;
-    }
-    unsigned tot;
-    const unsigned off = block_exscan<BLOCK>(S, deg, tot);
-    S.it_off[tid] = off;
-    __syncthreads();
-    /* the entry step staged up to BLOCK pushes: keep a round's worth of room */
-    if (S.pcnt > PSmem<BLOCK>::SB - PSmem<BLOCK>::U * BLOCK - BLOCK) flush<BLOCK>(P, c, S);
-    expand<FLT, BLOCK>(P, c, S, Q, k, tot, d_base);
+    if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
   }
-  flush<BLOCK>(P, c, S);
+  flush<BLOCK, UU>(P, c, S);
 }
 
 /* ------------------------------------------------------------------------ */
 /* The leader's decision (warp 0 of the last CTA to reach the barrier): what
  * the group runs next.  Replaces the assign manager's bucket advance and
  * termination logic (wl.h:851-1527) with a read of the list tails. */
-template <bool FLT, int BLOCK>
-__device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
+template <bool FLT, int BLOCK, int UU>
+__device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   const unsigned lane = threadIdx.x & 31u;
   PhGroup *G = grp_of(P, c);
-  const unsigned prev_mode = S.D.mode, prev_q = S.D.q;
+  const unsigned prev_mode = S.D.mode, prev_q = S.D.q, prev_list = S.D.list,
+                 prev_epoch = S.D.epoch;
+  bool hub_only = false;
   unsigned mode = PH_M_EXIT, q = prev_q, list = 0, base = ld_rlx32(&G->base);
   unsigned long long lo = 0, hi = 0;
   bool decide = false, next_query = false;
@@ -573,12 +719,15 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
     __syncwarp();
     base = 0u;
     decide = true;
-  } else if (prev_mode != PH_M_HUB && ld_rlx32(&G->hub_count) != 0u) {
+  } else if ((prev_mode == PH_M_LIGHT || prev_mode == PH_M_HEAVY) &&
+             ld_rlx32(&G->hub_claim) < ld_rlx32(&G->hub_count)) {
+    /* a solo phase left split-row records: the group expands them */
     mode = PH_M_HUB;
-    lo = 0;
+    list = prev_list;
+    lo = ld_rlx32(&G->hub_claim);
     hi = min(ld_rlx32(&G->hub_count), P.hub_cap);
+    hub_only = true;
   } else {
-    if (prev_mode == PH_M_HUB && lane == 0) st_rlx32(&G->hub_count, 0u);
     decide = true;
   }
   if (decide) {
@@ -622,7 +771,11 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
         next_query = true;
       }
     }
-    if ((mode == PH_M_LIGHT || mode == PH_M_HEAVY) && lane == 0) st_rlx64(&G->head[list], hi);
+    if ((mode == PH_M_LIGHT || mode == PH_M_HEAVY) && lane == 0) {
+      st_rlx64(&G->head[list], hi);
+      st_rlx32(&G->hub_count, 0u); /* split rows of the coming phase */
+      st_rlx32(&G->hub_claim, 0u);
+    }
   }
   if (next_query) {
     unsigned qi = 0;
@@ -650,7 +803,24 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
     }
   }
   const unsigned long long wb = ld_rlx64(&G->work);
+  unsigned epoch = prev_epoch; /* a records-only phase keeps its producer's */
+  if (lane == 0 && !hub_only) {
+    epoch = ld_rlx32(&G->epoch) + 1u;
+    if (epoch == 0u) epoch = 1u; /* 0 is what a cleared record sequence holds */
+    st_rlx32(&G->epoch, epoch);
+  }
   __syncwarp();
+  if (lane == 0 && P.trace && c.gi == 0u) {
+    const unsigned long long i = atomicAdd(&P.g->st_trace, 1ull);
+    if (i < P.trace_cap) {
+      PhTrace tr;
+      tr.t_ns = gtimer();
+      tr.count = mode == PH_M_INIT ? P.qs[q].n : (unsigned)min(hi - lo, 0xFFFFFFFFull);
+      tr.mode = (unsigned short)mode;
+      tr.base = (unsigned short)base;
+      P.trace[i] = tr;
+    }
+  }
   if (lane == 0) {
     S.D.mode = mode;
     S.D.q = q;
@@ -659,25 +829,33 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK> &S) {
     S.D.lo = lo;
     S.D.hi = hi;
     S.D.work_base = wb;
-    S.D.catchall = 0u;
+    S.D.epoch = epoch;
+    /* entries per claim: BLOCK, or fewer (a multiple of 32) so that a medium
+     * frontier reaches every CTA of the group */
+    const unsigned long long spread = (hi - lo + P.gsize - 1ull) / P.gsize;
+    S.D.per = (unsigned)min((unsigned long long)BLOCK, max(32ull, (spread + 31ull) & ~31ull));
   }
 }
 
 /* frontiers small enough for the leader alone */
-template <int BLOCK>
-__device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK> &S) {
+template <int BLOCK, int UU>
+__device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK, UU> &S) {
   const unsigned mode = S.D.mode;
   if (mode == PH_M_LIGHT || mode == PH_M_HEAVY) return S.D.hi - S.D.lo <= P.solo_max;
-  if (mode == PH_M_HUB) return S.D.hi - S.D.lo <= 1ull;
+  if (mode == PH_M_HUB) return false; /* left by a solo phase because it is large */
   if (mode == PH_M_INIT) return P.qs[S.D.q].n <= 64u * BLOCK;
   return false;
 }
 
 /* ------------------------------------------------------------------------ */
+/* edges in flight per thread: 8 where a thread may hold 128 registers, 4 at 64 */
+#define PH_U(BLOCK, MINB) ((BLOCK) * (MINB) >= 1024 ? 4 : 8)
+
 template <bool FLT, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constant__ PhParams P) {
+  constexpr int UU = PH_U(BLOCK, MINB);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  PSmem<BLOCK> &S = *reinterpret_cast<PSmem<BLOCK> *>(smem_raw);
+  PSmem<BLOCK, UU> &S = *reinterpret_cast<PSmem<BLOCK, UU> *>(smem_raw);
   const unsigned tid = threadIdx.x;
   Ctx c;
   c.gi = blockIdx.x / P.gsize;
@@ -699,7 +877,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   __syncthreads();
   for (;;) {
     const long long t0 = clock64();
-    run_phase<FLT, BLOCK>(P, c, S, false);
+    run_phase<FLT, BLOCK, UU>(P, c, S, false);
     const long long t1 = clock64();
     cy_work += (unsigned long long)(t1 - t0);
     /* group barrier: the last CTA in becomes the leader */
@@ -716,17 +894,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     __syncthreads();
     if (S.leader) {
       for (;;) {
-        if (tid < 32) leader_step<FLT, BLOCK>(P, c, S);
+        if (tid < 32) leader_step<FLT, BLOCK, UU>(P, c, S);
         __syncthreads();
         ++nphase;
-        if (!solo_ok<BLOCK>(P, S)) break;
-        if (tid == 0) ++S.st_solo;
-        run_phase<FLT, BLOCK>(P, c, S, true);
+        if (!solo_ok<BLOCK, UU>(P, S)) break;
+        if (tid == 0) {
+          st_rlx32(&G->producers, 1u); /* this CTA alone expands the phase */
+          __threadfence();
+          __threadfence();
+          ++S.st_solo;
+          if (P.trace && c.gi == 0u) { /* mark the record just written as solo */
+            const unsigned long long i = ld_rlx64(&P.g->st_trace) - 1ull;
+            if (i < P.trace_cap) P.trace[i].mode |= 0x100;
+          }
+        }
+        run_phase<FLT, BLOCK, UU>(P, c, S, true);
         __syncthreads();
         if (tid == 0) __threadfence();
         __syncthreads();
       }
       if (tid == 0) {
+        /* a records-only phase has no producers */
+        st_rlx32(&G->producers, S.D.mode == PH_M_HUB ? 0u : P.gsize);
         G->desc[(S.gen + 1u) & 1u] = S.D;
         __threadfence();
         st_rel32(&G->gen, S.gen + 1u);
@@ -751,6 +940,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
           S.D.lo = ld_rlx64(&dp->lo);
           S.D.hi = ld_rlx64(&dp->hi);
           S.D.work_base = ld_rlx64(&dp->work_base);
+          S.D.per = ld_rlx32(&dp->per);
+          S.D.epoch = ld_rlx32(&dp->epoch);
         } else {
           S.D.mode = PH_M_EXIT;
         }
@@ -785,7 +976,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
 
 template <bool FLT, int BLOCK, int MINB>
 static cudaError_t prep_one(int *max_blocks_per_sm) {
-  const size_t smem = sizeof(PSmem<BLOCK>);
+  const size_t smem = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
   cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -800,7 +991,7 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P.groups * P.gsize);
   cfg.blockDim = dim3(BLOCK);
-  cfg.dynamicSmemBytes = sizeof(PSmem<BLOCK>);
+  cfg.dynamicSmemBytes = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -813,9 +1004,9 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
 }  // namespace adds_phase
 
 /* Kernel variants: (threads per CTA, CTAs per SM the registers are sized
- * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1, 3: 512 x 1 (128
- * registers per thread), 4: 256 x 2 (128 registers). */
-#define PH_VARIANTS(X) X(0, 256, 4) X(1, 512, 2) X(2, 1024, 1) X(3, 512, 1) X(4, 256, 2)
+ * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1 (64 registers per
+ * thread), 3: 256 x 2, 4: 512 x 1 (128 registers per thread). */
+#define PH_VARIANTS(X) X(0, 256, 4) X(1, 512, 2) X(2, 1024, 1) X(3, 256, 2) X(4, 512, 1)
 
 int adds_phase_variant_block(int variant) {
 #define X(i, b, m) if (variant == i) return b;
@@ -856,7 +1047,7 @@ static unsigned ph_log2_ceil(unsigned long long x) {
 }
 
 void ph_engine_free(PhEngine &E) {
-  void *ptrs[] = {E.grp, E.g, E.qs, E.order, E.pool, E.pt, E.hub};
+  void *ptrs[] = {E.grp, E.g, E.qs, E.order, E.pool, E.pt, E.hub, E.hub_seq, E.trace};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (E.g_host) cudaFreeHost(E.g_host);
@@ -870,6 +1061,7 @@ int ph_engine_reset(PhEngine &E, cudaStream_t st) {
       cudaMemsetAsync(E.pt, 0xFF, ((size_t)E.groups * PH_NLIST << E.ptn_log2) * 8, st) !=
           cudaSuccess ||
       cudaMemsetAsync(E.g, 0, sizeof(PhGlobal), st) != cudaSuccess ||
+      cudaMemsetAsync(E.hub_seq, 0, (size_t)E.groups * E.hub_cap * 4, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return -5; /* ADDS_ERR_CUDA */
   return 0;
@@ -924,8 +1116,12 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
   if (pages > 0x3FFFFFFFull) return -4; /* ADDS_ERR_OOM */
   E.pages_per_group = (unsigned)pages;
   E.ptn_log2 = ph_log2_ceil(pages + 2ull);
+  /* records per phase: a split row of d edges gives ceil(d / chunk) <= d /
+   * chunk + 1 of them and only rows longer than the threshold (>= chunk) are
+   * split; a vertex can be expanded twice in one phase */
+  E.hub_eff = ph_hub_chunk(k);
   E.hub_cap = (unsigned)std::min<unsigned long long>(
-      0x7FFFFFFFull, 2ull * (mmax / std::max(64u, k.hub_chunk)) + 4096ull);
+      0x7FFFFFFFull, (4ull * (mmax / E.hub_eff) + 4096ull) * grow);
   E.qs_host = qv;
 #define PH_ALLOC(ptr, bytes_)                               \
   do {                                                      \
@@ -944,6 +1140,7 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
   PH_ALLOC(E.pool, (size_t)E.groups * E.pages_per_group * PH_PAGE * 8);
   PH_ALLOC(E.pt, ((size_t)E.groups * PH_NLIST << E.ptn_log2) * 8);
   PH_ALLOC(E.hub, (size_t)E.groups * E.hub_cap * sizeof(PhHub));
+  PH_ALLOC(E.hub_seq, (size_t)E.groups * E.hub_cap * 4);
 #undef PH_ALLOC
   if (cudaMallocHost((void **)&E.g_host, sizeof(PhGlobal)) != cudaSuccess) {
     cudaGetLastError();
@@ -965,6 +1162,11 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
   return ph_engine_reset(E, st);
 }
 
+unsigned ph_hub_chunk(const PhKnobs &k) {
+  const unsigned thr = std::max(64u, k.hub_threshold);
+  return std::max(64u, std::min(k.hub_chunk, thr));
+}
+
 int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P) {
   memset(P, 0, sizeof *P);
   P->qs = E.qs;
@@ -979,13 +1181,31 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->pt = E.pt;
   P->ptn_log2 = E.ptn_log2;
   P->hub = E.hub;
+  P->hub_seq = E.hub_seq;
   P->hub_cap = E.hub_cap;
   P->hub_threshold = std::max(64u, k.hub_threshold);
-  P->hub_chunk = std::max(64u, std::min(k.hub_chunk, P->hub_threshold));
+  P->hub_chunk = ph_hub_chunk(k);
+  if (P->hub_chunk < E.hub_eff) return -9; /* engine sized for longer chunks */
   P->solo_max = k.solo_max;
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;
+  P->trace = E.trace;
+  P->trace_cap = E.trace_cap;
+  return 0;
+}
+
+/* Turns the phase trace of group 0 on (cap > 0, allocates) or off. */
+int ph_engine_trace(PhEngine &E, unsigned cap) {
+  if (E.trace) cudaFree(E.trace);
+  E.trace = nullptr;
+  E.trace_cap = 0;
+  if (cap == 0) return 0;
+  if (cudaMalloc((void **)&E.trace, (size_t)cap * sizeof(PhTrace)) != cudaSuccess) {
+    cudaGetLastError();
+    return -4;
+  }
+  E.trace_cap = cap;
   return 0;
 }
 

@@ -35,7 +35,7 @@
 #define PH_M_INIT 0u   /* fill the query's distances with INF                 */
 #define PH_M_LIGHT 1u  /* expand light edges of a list range                  */
 #define PH_M_HEAVY 2u  /* expand heavy edges of settled vertices              */
-#define PH_M_HUB 3u    /* expand split-row chunks                             */
+#define PH_M_HUB 3u    /* (reserved: split rows are expanded inside their phase) */
 #define PH_M_EXIT 4u   /* no more queries for this group                      */
 
 /* device error codes (first one wins) */
@@ -72,8 +72,9 @@ struct __align__(64) PhDesc {
   unsigned base;               /* absolute bucket being settled              */
   unsigned long long lo, hi;   /* entry range of the list (hub: record range) */
   unsigned long long work_base; /* claim counter value at phase start        */
-  unsigned catchall;           /* the range may hold entries of later buckets */
-  unsigned pad[5];
+  unsigned per;                /* entries per claim                           */
+  unsigned epoch;              /* phase number: marks its split-row records    */
+  unsigned pad[4];
 };
 
 /* Per-group state.  `arrive` and `gen` sit in lines of their own; the list
@@ -91,8 +92,12 @@ struct __align__(128) PhGroup {
   unsigned pad1[31];
   unsigned long long work;     /* chunk claim counter (monotone)             */
   unsigned long long pad2[15];
-  unsigned hub_count;          /* split-row chunks appended this phase       */
+  unsigned hub_count;          /* split-row records appended this phase      */
   unsigned pad3[31];
+  unsigned hub_claim;          /* split-row records claimed this phase       */
+  unsigned pad3b[31];
+  unsigned producers;          /* CTAs that may still append records         */
+  unsigned pad3c[31];
   unsigned page_next;          /* bump allocator: next free page (relative)  */
   unsigned pad4[31];
   PhDesc desc[2];
@@ -100,7 +105,8 @@ struct __align__(128) PhGroup {
   unsigned q;                  /* current query                              */
   unsigned base;               /* absolute base bucket                       */
   unsigned mode;               /* mode of the phase that just ran            */
-  unsigned pad5[29];
+  unsigned epoch;              /* phases decided so far                      */
+  unsigned pad5[28];
   unsigned long long head[PH_NLIST];
   PhTail tails[PH_NLIST];
 };
@@ -116,7 +122,17 @@ struct __align__(128) PhGlobal {
       st_phases, st_solo, st_heavy, st_repush, st_pages;
   unsigned long long st_cyc[4]; /* SM cycles summed over CTAs: work, barrier
                                    wait, leader, total                        */
-  unsigned long long st_pad[1];
+  unsigned long long st_trace;  /* trace records written (may exceed the cap) */
+  unsigned long long st_direct; /* pushes that bypassed a full staging buffer */
+};
+
+/* One record of the phase trace (group 0 only): when the leader decided a
+ * phase, what it was and how big. */
+struct PhTrace {
+  unsigned long long t_ns;  /* %globaltimer at the decision                  */
+  unsigned count;           /* entries (hub: chunk records; init: vertices)   */
+  unsigned short mode;      /* PH_M_* | 0x100 if run by the leader alone      */
+  unsigned short base;      /* low 16 bits of the base bucket                 */
 };
 
 /* Kernel parameters (by value). */
@@ -133,6 +149,7 @@ struct PhParams {
   unsigned long long *pt;      /* groups * PH_NLIST << ptn_log2 cells         */
   unsigned ptn_log2;
   PhHub *hub;                  /* groups * hub_cap records                    */
+  unsigned *hub_seq;           /* groups * hub_cap: epoch of each written record */
   unsigned hub_cap;
   unsigned hub_threshold;      /* rows with more expanded edges are split     */
   unsigned hub_chunk;          /* edges per split chunk                       */
@@ -140,6 +157,8 @@ struct PhParams {
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
+  PhTrace *trace;              /* optional phase trace of group 0              */
+  unsigned trace_cap;
 };
 
 #ifdef __cplusplus
@@ -152,13 +171,17 @@ struct PhEngine {
   bool flt = false;
   unsigned nq = 0, groups = 0, gsize = 0, block = 0, variant = 0;
   unsigned pages_per_group = 0, ptn_log2 = 0, hub_cap = 0, max_n = 0;
+  unsigned hub_eff = 0; /* split-row chunk length the record store is sized for */
   PhGroup *grp = nullptr;
   PhGlobal *g = nullptr;
   PhQuery *qs = nullptr;
   unsigned *order = nullptr;
   unsigned long long *pool = nullptr, *pt = nullptr;
   PhHub *hub = nullptr;
+  unsigned *hub_seq = nullptr;
   PhGlobal *g_host = nullptr; /* pinned copy of the statistics and error word */
+  PhTrace *trace = nullptr;    /* phase trace buffer (allocated on request)  */
+  unsigned trace_cap = 0;
   std::vector<PhQuery> qs_host;
   size_t bytes = 0;
   int num_sms = 0;
@@ -186,6 +209,8 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
 int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent_t k0,
                       cudaEvent_t k1);
 int ph_engine_status(const PhEngine &E, char *msg, size_t msg_len);
+int ph_engine_trace(PhEngine &E, unsigned cap);
+unsigned ph_hub_chunk(const PhKnobs &k); /* effective split-row chunk length */
 #endif
 
 #endif /* ADDS_PHASE_INTERNAL_H_ */

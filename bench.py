@@ -236,9 +236,10 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
         A.check(A.lib().adds_graph_download(g.handle, csr_row.ctypes.data, None, None))
     srcs = pick_sources(g, wl, csr_row)
     tuned, tune_ms = None, None
+    extra_opts = json.loads(args.opts) if args.opts else {}
     if not args.no_tune:
         tuned, tune_ms = g.tune(srcs[:2], A.default_opts(engine=args.engine))
-    opts = A.default_opts(timeout_ms=60000, engine=args.engine)
+    opts = A.default_opts(timeout_ms=60000, engine=args.engine, **extra_opts)
     # per-source reached vertices / edges (outside the timed region)
     mr, nr = {}, {}
     for s in srcs:
@@ -298,6 +299,12 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
            "note": "adds_sssp(graph, src, pinned host dist) per step, host wall clock; the "
                    "4-byte source id is the step input, the distance array the result"}
     work_edges = st["edges_scanned"]
+    if args.trace:  # one more solve with the phase trace on (outside the timed region)
+        g.trace(1 << 16)
+        g.sssp(steps[0], opts)
+        tr, ntr = g.trace_read(1 << 16)
+        g.trace(0)
+        np.save(args.trace, tr)
     out = {
         "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps * 1e3,
@@ -582,6 +589,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--engine", type=int, default=0, help="0 auto, 1 async, 2 phase")
+    ap.add_argument("--opts", default="", help="JSON dict of adds_opts fields to override")
+    ap.add_argument("--trace", default="", help="save the phase trace of one solve (.npy)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -266,6 +266,25 @@ int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_start,
                       const uint32_t *edges, adds_wtype wt, uint32_t src,
                       uint32_t *dist, void *stream);
 
+/* ---- phase trace (diagnostics) ------------------------------------------ */
+/* One record per phase the phase engine decided, in order (the leader's
+ * %globaltimer at the decision; a phase lasts until the next record).
+ * Extends the reference's per-run work record (ads_int/kernel.cu:264-282)
+ * down to the phase; the reference has no tracing of its own. */
+typedef struct adds_phase_trace {
+  uint64_t t_ns;  /* device clock at the decision, ns                       */
+  uint32_t count; /* frontier entries (split rows: chunks; init: vertices)   */
+  uint16_t mode;  /* 0 init, 1 light, 2 heavy, 3 split rows, 4 exit;
+                     | 0x100 when one CTA ran it alone                      */
+  uint16_t base;  /* low 16 bits of the bucket being settled                */
+} adds_phase_trace;
+/* Records up to cap phases of each later plain solve on g (0 = off). */
+int adds_graph_trace(adds_graph *g, uint32_t cap);
+/* Copies the last solve's records (at most cap) to host memory; *written
+ * receives how many the solve produced (it may exceed the capacity). */
+int adds_graph_trace_read(adds_graph *g, adds_phase_trace *out, uint32_t cap,
+                          uint64_t *written);
+
 /* ---- autotuner ---------------------------------------------------------- */
 /* Times candidate settings on the sample sources and stores the fastest in
  * the graph (used whenever a later call passes "auto" knobs): delta, then for
