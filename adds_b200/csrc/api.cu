@@ -1057,7 +1057,9 @@ static void fill_phase_stats(const PhEngine &E, adds_stats *s) {
   s->batches = g.st_chunks;
   s->hub_chunks = g.st_hub;
   s->heavy_lists = g.st_heavy;
-  for (int i = 0; i < 4; ++i) s->phase_cycles[i] = g.st_cyc[i];
+  for (int i = 0; i < 6; ++i) s->phase_cycles[i] = g.st_cyc[i];
+  s->mid_flush_cycles = g.st_cyc[6]; /* grid-phase work */
+  s->mid_flushes = g.st_cyc[7];      /* total */
   s->ctas = (int32_t)(E.groups * E.gsize);
   s->engine = ADDS_ENGINE_PHASE;
   s->phases = g.st_phases;

@@ -156,6 +156,9 @@ struct PSmem {
   unsigned long long st_items, st_stale, st_heavy, st_repush, st_pushes, st_chunks, st_hubs,
       st_solo;
   unsigned long long claim;
+  unsigned long long cy[8]; /* thread 0's cycles: entry prep, record prep (with
+                               waits), expand, flush, barrier wait, leader,
+                               grid-phase work, total */
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
 };
 
@@ -553,18 +556,20 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
   return true;
 }
 
-/* Relaxes the chunk's edges: in iteration i thread t takes edges
- * i*BLOCK*U + u*BLOCK + t (u < U), so loads of neighbouring threads are
- * neighbours in memory; it issues the loads of iteration i+1 before the
- * distance gathers and atomicMins of iteration i.  Every SEGI iterations the
- * CTA meets once to flush staged pushes (the staging buffer is sized so that
- * this is the only barrier needed). */
+/* Relaxes the chunk's edges.  In iteration i warp w takes the 32*U edges
+ * i*BLOCK*U + w*32*U + [0, 32*U), lane l every 32nd of them, so each load
+ * instruction of a warp reads 32 neighbouring edges and a lane's successive
+ * edges are 32 apart: its item is found by a short forward (galloping)
+ * search from the previous one.  The loads of iteration i+1 are issued
+ * before the distance gathers of iteration i.  Every SEGI iterations the CTA
+ * meets once to flush staged pushes (the staging buffer is sized so that this
+ * is the only barrier needed). */
 template <bool FLT, int BLOCK, int UU>
 __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q,
                        unsigned base) {
   constexpr int U = PSmem<BLOCK, UU>::U;
   constexpr unsigned R = BLOCK * U;
-  const unsigned tid = threadIdx.x;
+  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const unsigned k = S.ck_k, E = S.ck_E;
   const unsigned nit = (E + R - 1u) / R; /* the same for every thread */
   const uint2 *__restrict__ edges = Q.edges;
@@ -572,27 +577,38 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   const float scale = Q.scale;
   const unsigned shift = Q.shift;
   const unsigned long long pol = evict_first_policy();
-  int lo = 0; /* a thread's edges only move forward: searches start at the last item */
+  const unsigned *off = S.it_off; /* off[k] = E */
+  unsigned lo = 0; /* item of the thread's last edge: its edges only move forward */
   uint2 ne[U];
   unsigned nu[U];
+  auto find = [&](unsigned e) {
+    /* gallop: the last item whose offset is <= e, at or after lo */
+    unsigned step = 1u;
+    while (lo + step < k && off[lo + step] <= e) {
+      lo += step;
+      step <<= 1;
+    }
+    unsigned hi = min(lo + step, k) - 1u; /* off[hi + 1] > e or hi = k - 1 */
+    while (lo < hi) {
+      const unsigned mid = (lo + hi + 1u) >> 1;
+      if (off[mid] <= e) lo = mid; else hi = mid - 1u;
+    }
+  };
   auto load_round = [&](unsigned eb) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const unsigned e = eb + u * BLOCK;
+      const unsigned e = eb + u * 32u;
       nu[u] = 0xFFFFFFFFu;
       ne[u] = make_uint2(0u, 0u);
       if (e < E) {
-        int hi = (int)k - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (S.it_off[mid] <= e) lo = mid; else hi = mid - 1;
-        }
-        ne[u] = ld_edge(edges + S.it_rb[lo] + (e - S.it_off[lo]), pol);
+        find(e);
+        ne[u] = ld_edge(edges + S.it_rb[lo] + (e - off[lo]), pol);
         nu[u] = S.it_du[lo];
       }
     }
   };
-  if (nit) load_round(tid);
+  const unsigned mine = warp * 32u * U + lane; /* offset of the thread's first edge */
+  if (nit) load_round(mine);
   unsigned nedges = 0;
   for (unsigned it = 0; it < nit; ++it) {
     unsigned dst[U], nd[U], cur[U];
@@ -606,7 +622,7 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
         ++nedges;
       }
     }
-    if (it + 1u < nit) load_round((it + 1u) * R + tid);
+    if (it + 1u < nit) load_round((it + 1u) * R + mine);
 #pragma unroll
     for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
     /* an improvement on the gathered value is applied with a reduction (no
@@ -623,7 +639,11 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
     }
     if ((it % PSmem<BLOCK, UU>::SEGI) == PSmem<BLOCK, UU>::SEGI - 1u || it + 1u == nit) {
       __syncthreads();
-      if (S.pcnt > (unsigned)PSmem<BLOCK, UU>::FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+      if (S.pcnt > (unsigned)PSmem<BLOCK, UU>::FLUSH_AT) {
+        const long long f0 = clock64();
+        flush<BLOCK, UU>(P, c, S);
+        if (tid == 0) S.cy[3] += (unsigned long long)(clock64() - f0); /* also in expand's */
+      }
     }
   }
   c.edges += nedges;
@@ -658,9 +678,15 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
   /* frontier chunks first, then split-row records (a records-only phase
    * finishes what a solo phase left) */
   bool records = mode == PH_M_HUB;
+  long long t0 = clock64();
   for (;;) {
     const bool have = records ? prepare_records<FLT, BLOCK, UU>(P, c, S)
                               : prepare_chunk<FLT, BLOCK, UU>(P, c, S, solo, local_claim, pend);
+    {
+      const long long t1 = clock64();
+      if (tid == 0) S.cy[records ? 1 : 0] += (unsigned long long)(t1 - t0);
+      t0 = t1;
+    }
     if (!have) {
       if (records) break;
       /* no frontier chunk left for this CTA: it appends no more split rows,
@@ -680,9 +706,20 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
     }
     if (S.ck_E != 0u) expand<FLT, BLOCK, UU>(P, c, S, Q, base);
     __syncthreads();
+    {
+      const long long t1 = clock64();
+      if (tid == 0) S.cy[2] += (unsigned long long)(t1 - t0);
+      t0 = t1;
+    }
     if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+    {
+      const long long t1 = clock64();
+      if (tid == 0) S.cy[3] += (unsigned long long)(t1 - t0);
+      t0 = t1;
+    }
   }
   flush<BLOCK, UU>(P, c, S);
+  if (tid == 0) S.cy[3] += (unsigned long long)(clock64() - t0);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -872,6 +909,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     S.D.q = 0u;
     S.st_items = S.st_stale = S.st_heavy = S.st_repush = S.st_pushes = S.st_chunks = 0;
     S.st_hubs = S.st_solo = 0;
+    for (int i = 0; i < 8; ++i) S.cy[i] = 0ull;
   }
   if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
@@ -967,10 +1005,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     atomicAdd(&g->st_hub, S.st_hubs);
     atomicAdd(&g->st_solo, S.st_solo);
     atomicAdd(&g->st_phases, nphase);
-    atomicAdd(&g->st_cyc[0], cy_work);
-    atomicAdd(&g->st_cyc[1], cy_wait);
-    atomicAdd(&g->st_cyc[2], cy_lead);
-    atomicAdd(&g->st_cyc[3], (unsigned long long)(clock64() - cy0));
+    S.cy[4] = cy_wait;
+    S.cy[5] = cy_lead;
+    S.cy[6] = cy_work; /* run_phase as a whole, grid phases */
+    S.cy[7] = (unsigned long long)(clock64() - cy0);
+    for (int i = 0; i < 8; ++i) atomicAdd(&g->st_cyc[i], S.cy[i]);
   }
 }
 

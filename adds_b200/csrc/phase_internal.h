@@ -120,8 +120,11 @@ struct __align__(128) PhGlobal {
   unsigned pad1[31];
   unsigned long long st_items, st_stale, st_edges, st_pushes, st_chunks, st_hub,
       st_phases, st_solo, st_heavy, st_repush, st_pages;
-  unsigned long long st_cyc[4]; /* SM cycles summed over CTAs: work, barrier
-                                   wait, leader, total                        */
+  unsigned long long st_cyc[8]; /* SM cycles summed over CTAs: entry chunk
+                                   preparation, record preparation (with its
+                                   waits), expansion, flushes, barrier wait,
+                                   leader (solo phases included), grid-phase
+                                   work, total                                */
   unsigned long long st_trace;  /* trace records written (may exceed the cap) */
   unsigned long long st_direct; /* pushes that bypassed a full staging buffer */
 };

@@ -8,7 +8,7 @@ out-degree > 0.  A step is one solve from the next source.  Metric: GTEPS =
 out-edges of the reached vertices / solve time (the Graph500 convention).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload rmat24|rmat16|grid4096|rmat26|batched|diff]
+                  [--workload rmat24|rmat16|rmat21|rmat22|grid4096|rmat26|batched|diff]
 
 --impl reference times the reference's CPU delta-stepping path (Galois
 OBIM delta-stepping, restated in oracle/oracle.c because Galois is not
@@ -106,6 +106,7 @@ WORKLOADS = {
     "rmat16": dict(kind="rmat", scale=16, wtype=0, w_lo=1, w_hi=1000, nsrc=1, seed=16,
                    src="maxdeg"),
     "rmat21": dict(kind="rmat", scale=21, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=21),
+    "rmat22": dict(kind="rmat", scale=22, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=22),
     "grid4096": dict(kind="grid", side=4096, wtype=1, w_lo=1.0, w_hi=100.0, nsrc=1, seed=4096,
                      src="center"),
 }
@@ -329,7 +330,8 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
             "items_last": st["items_popped"], "stale_last": st["items_stale"],
             "pushes_last": st["pushes"], "ctas": st["ctas"], "engine": st["engine"],
             "phases_last": st["phases"], "solo_phases_last": st["solo_phases"],
-            "chunks_last": st["batches"], "phase_cycles_last": st["phase_cycles"],
+            "chunks_last": st["batches"],
+            "phase_cycles_last": st["phase_cycles"] + [st["mid_flush_cycles"], st["mid_flushes"]],
             "tuned": ({k: getattr(tuned, k) for k in ("engine", "delta_shift", "block_threads",
                                                         "ctas_per_sm", "solo_max",
                                                         "hub_threshold", "light_heavy", "window",

@@ -100,15 +100,20 @@ typedef struct adds_stats {
   uint64_t items_stale;     /* popped entries skipped as superseded            */
   uint64_t edges_scanned;   /* edges of expanded vertices (float work count)   */
   uint64_t pushes;          /* queue entries pushed                            */
-  uint64_t batches;         /* CTA-level pops                                  */
+  uint64_t batches;         /* CTA-level pops (phase engine: frontier chunks)  */
   uint64_t hub_chunks;      /* split row chunks processed                      */
   uint64_t hub_stale;       /* of which skipped (row's vertex had improved)    */
   uint64_t local_batches;   /* batches a CTA took from its own pushes          */
   uint64_t heavy_lists;     /* settled vertices whose heavy edges were relaxed */
-  uint64_t phase_cycles[6]; /* SM cycles summed over CTAs: acquire, load,
-                               edges, flush, idle, total                      */
-  uint64_t mid_flush_cycles; /* of the edge phase: flushes of a full buffer   */
-  uint64_t mid_flushes;
+  uint64_t phase_cycles[6]; /* SM cycles summed over CTAs.  Async engine:
+                               acquire, load, edges, flush, idle, total.
+                               Phase engine: chunk preparation, split-row
+                               record preparation (waits included), edge
+                               expansion, flushes, group-barrier wait, leader
+                               (solo phases included)                         */
+  uint64_t mid_flush_cycles; /* async: edge-phase flushes of a full buffer;
+                                phase: cycles in grid phases                  */
+  uint64_t mid_flushes;     /* async: their count; phase: total cycles        */
   uint64_t reached;         /* vertices with finite distance (filled on request) */
   uint64_t reached_edges;   /* out-edges of reached vertices (filled on request) */
   int32_t delta_shift;      /* bucket shift at the end of the solve            */
