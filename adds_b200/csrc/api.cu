@@ -1629,26 +1629,44 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   int rc = set_device(g->device);
   if (rc) return rc;
   g->tuned = 0;
-  adds_opts cur;
-  adds_opts_init(&cur);
-  if (best && best->engine > 0) cur.engine = best->engine; /* in: engine to tune */
+  /* the defaults of one engine, every knob spelled out */
   Knobs k;
   int s0;
   float sc;
-  resolve(g, &cur, &k, &s0, &sc);
-  cur.delta_shift = s0;
-  cur.delta_scale = sc;
-  cur.window = k.window;
-  cur.batch_max = k.batch_max;
-  cur.hub_threshold = k.hub_threshold;
-  cur.strict_order = k.strict;
-  cur.local_max = k.local_max;
-  cur.light_heavy = k.light_heavy;
-  cur.block_threads = k.block;
-  cur.greed = k.greed;
-  cur.engine = k.engine;
-  cur.solo_max = k.solo_max;
+  auto defaults = [&](int engine) {
+    adds_opts o;
+    adds_opts_init(&o);
+    o.engine = engine;
+    resolve(g, &o, &k, &s0, &sc);
+    o.delta_shift = s0;
+    o.delta_scale = sc;
+    o.window = k.window;
+    o.batch_max = k.batch_max;
+    o.hub_threshold = k.hub_threshold;
+    o.strict_order = k.strict;
+    o.local_max = k.local_max;
+    o.light_heavy = k.light_heavy;
+    o.block_threads = k.block;
+    o.greed = k.greed;
+    o.engine = k.engine;
+    o.solo_max = k.solo_max;
+    return o;
+  };
+  /* in: the engine to tune; auto times both and tunes the faster one (the
+   * phase engine wins on low-diameter graphs, the asynchronous one where
+   * thousands of buckets each hold a thin frontier) */
+  const int want = (best && best->engine > 0) ? best->engine : ADDS_ENGINE_AUTO;
+  adds_opts cur = defaults(want == ADDS_ENGINE_ASYNC ? ADDS_ENGINE_ASYNC : ADDS_ENGINE_PHASE);
   double bm = time_solves(g, srcs, ns, &cur);
+  if (want == ADDS_ENGINE_AUTO) {
+    const adds_opts alt = defaults(ADDS_ENGINE_ASYNC);
+    const double ma = time_solves(g, srcs, ns, &alt);
+    if (ma < bm) {
+      bm = ma;
+      cur = alt;
+    }
+  }
+  resolve(g, &cur, &k, &s0, &sc); /* knobs of the chosen engine */
   auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
     for (int v : vals) {
       if (v == cur.*f) continue;
@@ -1665,7 +1683,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   for (int d = -4; d <= 4; ++d)
     if (s0 + d >= 0 && s0 + d <= 31) shifts.push_back(s0 + d);
   try_field(&adds_opts::delta_shift, shifts);
-  if (k.engine == ADDS_ENGINE_PHASE) {
+  if (cur.engine == ADDS_ENGINE_PHASE) {
     /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
     const int combos[5][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}};
     for (const auto &cb : combos) {

@@ -281,7 +281,8 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
     balg = sum(12 * mr[s] + 24 * nr[s] for s in steps)
     peak, peak_kind = measured_peaks()
     achieved = balg / kernel_s / 1e9
-    prof = profile_traffic(f"solve_kernel_{wl_name}")
+    kname = "phase_kernel" if st["engine"] == 2 else "solve_kernel"
+    prof = profile_traffic(f"{kname}_{wl_name}")
     traffic = None
     if prof and "dram_bytes_per_launch" in prof:
         traffic = prof["dram_bytes_per_launch"]
@@ -316,7 +317,9 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
-                     "kernel": "adds::solve_kernel (persistent, 1 launch per solve)",
+                     "kernel": ("adds_phase::phase_kernel" if st["engine"] == 2 else
+                                "adds::solve_kernel") + " (persistent, 1 launch per solve)",
+                     "traffic_note": (prof or {}).get("scaled_by"),
                      "bytes_model": "12*m_r + 24*n_r per solve"},
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,

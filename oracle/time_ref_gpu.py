@@ -2,7 +2,7 @@
 oracle/build_ref.sh) against this engine on one workload of bench.py.
 TEST/MEASUREMENT INFRASTRUCTURE ONLY.  Needs a GPU.
 
-  python oracle/time_ref_gpu.py rmat24 [nsources] [out.json]
+  python oracle/time_ref_gpu.py rmat22 [nsources] [out.json] [timeout_s]
 
 For each source, the reference binary runs as the reference's run_all.sh
 does (`sssp -s src -o out graph.gr 3>record`); its fd-3 record gives the
@@ -29,6 +29,7 @@ def main():
     wl_name = sys.argv[1] if len(sys.argv) > 1 else "rmat24"
     nsrc = int(sys.argv[2]) if len(sys.argv) > 2 else 2
     out_json = sys.argv[3] if len(sys.argv) > 3 else None
+    tmo = int(sys.argv[4]) if len(sys.argv) > 4 else 120
     wl = bench.WORKLOADS[wl_name]
     g = bench.make_graph(wl, 0)
     row = np.empty(g.n + 1, dtype=np.uint64)
@@ -44,7 +45,7 @@ def main():
             g.sssp(s)
             nr, mr = g.reached()
             rec = os.path.join(tmp, "rec")
-            cmd = f'timeout 900 "{binary}" -s {s} "{gr}" 3>"{rec}" > "{tmp}/log" 2>&1'
+            cmd = f'timeout {tmo} "{binary}" -s {s} "{gr}" 3>"{rec}" > "{tmp}/log" 2>&1'
             r = subprocess.run(["bash", "-c", cmd])
             if r.returncode != 0:
                 res["sources"].append({"src": s, "error": f"exit {r.returncode}",
