@@ -275,6 +275,7 @@ struct Knobs {
 static int phase_variant(int block, int cps) {
   if (block == 1024) return 2;
   if (block == 512) return cps == 1 ? 4 : 1;
+  if (block == 128) return 5;
   return cps == 2 ? 3 : 0;
 }
 
@@ -1685,7 +1686,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
   try_field(&adds_opts::delta_shift, shifts);
   if (cur.engine == ADDS_ENGINE_PHASE) {
     /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
-    const int combos[5][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}};
+    const int combos[6][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}, {128, 8}};
     for (const auto &cb : combos) {
       adds_opts t = cur;
       t.block_threads = cb[0];

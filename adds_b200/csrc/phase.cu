@@ -124,6 +124,7 @@ __device__ __forceinline__ unsigned route(unsigned b, unsigned base) {
 /* ------------------------------------------------------------------------ */
 /* shared memory of one CTA                                                   */
 #define PH_RES_PAGES 6u /* pages one list reservation may touch (flush size) */
+#define PH_EPT 1        /* frontier entries one thread prepares per chunk     */
 /* split-row chunk records one CTA takes at a time */
 #define PH_HUB_PER_CLAIM(BLOCK) ((BLOCK) / 16u)
 
@@ -131,16 +132,18 @@ template <int BLOCK, int UU>
 struct PSmem {
   static constexpr int U = UU;      /* edges per thread in flight                     */
   static constexpr int SEGI = 2;    /* iterations of U edges between flush checks     */
-  static constexpr int FLUSH_AT = 4 * BLOCK; /* flush once more than this is staged  */
+  static constexpr int EPT = PH_EPT;         /* frontier entries per thread per chunk */
+  static constexpr int IC = EPT * BLOCK;     /* items per chunk                        */
+  static constexpr int FLUSH_AT = 2 * BLOCK; /* flush once more than this is staged  */
   /* staged pushes: FLUSH_AT, plus one per entry of a chunk, plus one per edge of
    * a segment -- a segment can never overflow the buffer */
-  static constexpr int SB = FLUSH_AT + BLOCK + SEGI * U * BLOCK;
+  static constexpr int SB = FLUSH_AT + IC + SEGI * U * BLOCK;
   static_assert(SB <= (int)((PH_RES_PAGES - 1u) * PH_PAGE + 1u),
                 "a flush must fit in PH_RES_PAGES pages of one list");
   /* the items of the chunk being expanded: row segments [rb, re) */
-  unsigned it_rb[BLOCK];
-  unsigned it_du[BLOCK];      /* distance the item is expanded with              */
-  unsigned it_off[BLOCK + 1]; /* exclusive scan of the segment lengths           */
+  unsigned it_rb[IC];
+  unsigned it_du[IC];      /* distance the item is expanded with                 */
+  unsigned it_off[IC + 1]; /* exclusive scan of the segment lengths              */
   unsigned ck_k, ck_E;        /* items and edges of the chunk                    */
   unsigned pb_v[SB];
   unsigned pb_d[SB];
@@ -370,23 +373,43 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
   const PhQuery &Q = P.qs[S.D.q];
   const unsigned long long d_lo = S.D.lo, d_hi = S.D.hi, d_wb = S.D.work_base;
   const unsigned d_base = S.D.base, d_list = S.D.list;
-  /* entries per claim: the leader spreads a medium frontier over every CTA */
-  const unsigned per = solo ? (unsigned)BLOCK : S.D.per;
+  constexpr unsigned IC = PSmem<BLOCK, UU>::IC;
+  const unsigned long long count = d_hi - d_lo;
   __syncthreads(); /* everyone has read the previous claim's S.stop */
   if (tid == 0) {
+    /* guided self-scheduling: a claim takes about half this CTA's share of
+     * what is left (at least 32 entries, at most IC), so a phase starts with
+     * large chunks and ends with small ones */
+    auto want = [&](unsigned long long seen) {
+      const unsigned long long left = count > seen ? count - seen : 0ull;
+      const unsigned long long w = (left / (2ull * P.gsize) + 31ull) & ~31ull;
+      return (unsigned)min((unsigned long long)IC, max(32ull, w));
+    };
+    unsigned long long at;
+    unsigned n;
     if (solo) {
-      S.claim = local_claim++;
+      at = local_claim;
+      n = IC;
+      local_claim += IC;
     } else {
       /* the next claim is taken one chunk ahead, so its latency overlaps this
-       * chunk's work; claims past the end are simply not used */
-      const unsigned long long cl = pend != ~0ull ? pend : atomicAdd(&G->work, 1ull);
-      pend = atomicAdd(&G->work, 1ull);
-      S.claim = cl - d_wb;
+       * chunk's work; claims past the end are simply not used.  pend packs
+       * the claim's start (entries since work_base, 40 bits) and size. */
+      if (pend == ~0ull) {
+        const unsigned w = want(0ull);
+        pend = ((atomicAdd(&G->work, (unsigned long long)w) - d_wb) << 24) | w;
+      }
+      at = pend >> 24;
+      n = (unsigned)(pend & 0xFFFFFFull);
+      const unsigned w = want(at + n);
+      pend = ((atomicAdd(&G->work, (unsigned long long)w) - d_wb) << 24) | w;
     }
-    S.stop = S.claim * per >= d_hi - d_lo ? 1u : 0u;
+    S.claim = at;
+    S.stop = at >= count ? 1u : 0u;
     if (!S.stop) {
-      const unsigned long long s0 = d_lo + S.claim * per;
-      const unsigned long long s1 = min(s0 + per, d_hi) - 1ull;
+      const unsigned long long s0 = d_lo + at;
+      const unsigned long long s1 = min(s0 + n, d_hi) - 1ull;
+      S.ck_k = (unsigned)(s1 + 1ull - s0);
       const unsigned long long v0 = s0 >> PH_PAGE_LOG2, v1 = s1 >> PH_PAGE_LOG2;
       S.pi0 = S.ptc_vp[d_list] == v0 ? S.ptc_pi[d_list] : pt_lookup(P, c, d_list, v0);
       S.pi1 = v1 == v0 ? S.pi0 : pt_lookup(P, c, d_list, v1);
@@ -398,74 +421,111 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
   }
   __syncthreads();
   if (S.stop) return false;
-  const unsigned long long s0 = d_lo + S.claim * per;
-  const unsigned k = (unsigned)min((unsigned long long)per, d_hi - s0);
-  unsigned rb = 0, re = 0, du = 0;
-  bool stale = false, repush = false;
-  if (tid < k) {
-    {
-      const unsigned long long idx = s0 + tid;
+  const unsigned long long s0 = d_lo + S.claim;
+  const unsigned k = S.ck_k;
+  constexpr int EPT = PSmem<BLOCK, UU>::EPT;
+  /* item i = j*BLOCK + tid: neighbouring threads read neighbouring entries;
+   * the loads of all EPT entries are issued before their dependants */
+  unsigned ev[EPT], ed[EPT], dv[EPT];
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    const unsigned i = j * BLOCK + tid;
+    ev[j] = 0xFFFFFFFFu;
+    ed[j] = 0u;
+    if (i < k) {
+      const unsigned long long idx = s0 + i;
       const unsigned pg = ((idx >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2)) ? S.pi0 : S.pi1;
       if (pg != 0xFFFFFFFFu) {
         const unsigned long long e = __ldcg(entry_ptr(P, c, pg, idx));
-        const unsigned v = (unsigned)e, d = (unsigned)(e >> 32);
-        if (__ldcg(Q.dist + v) != d) {
-          stale = true; /* superseded: a later push carries the smaller value */
-        } else {
-          const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
-          if (b > d_base) { /* left in the far slot: move it to its own bucket */
-            stage<BLOCK, UU>(S, v, d, route(b, d_base));
-            repush = true;
-          } else {
-            const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
-            const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
-            if (mode == PH_M_LIGHT) {
-              rb = r0;
-              re = r0 + nl;
-              if (nl < r1 - r0) stage<BLOCK, UU>(S, v, d, PH_LSETTLED);
-            } else {
-              rb = r0 + nl;
-              re = r1;
-            }
-            if (re - rb > P.hub_threshold) { /* cut into chunks for the whole group */
-              const unsigned deg = re - rb;
-              const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
-              const unsigned hb = atomicAdd(&G->hub_count, nch);
-              if (hb + nch > P.hub_cap) {
-                raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
-              } else {
-                PhHub *hp = hub_of(P, c) + hb;
-                unsigned *sq = hub_seq_of(P, c) + hb;
-                for (unsigned j = 0; j < nch; ++j)
-                  __stcg(reinterpret_cast<uint4 *>(hp + j),
-                         make_uint4(v, d, rb + j * P.hub_chunk,
-                                    rb + min(deg, (j + 1u) * P.hub_chunk)));
-                __threadfence(); /* the records before their sequence words */
-                const unsigned ep = S.D.epoch;
-                for (unsigned j = 0; j < nch; ++j) st_rlx32(sq + j, ep);
-              }
-              re = rb;
-            }
-            du = d;
-          }
-        }
+        ev[j] = (unsigned)e;
+        ed[j] = (unsigned)(e >> 32);
       }
     }
   }
-  S.it_rb[tid] = rb;
-  S.it_du[tid] = du;
-  const unsigned nstale = __syncthreads_count(stale);
-  const unsigned nrepush = __syncthreads_count(repush);
-  if (tid == 0) {
-    S.st_stale += nstale;
-    S.st_repush += nrepush;
-    if (mode == PH_M_HEAVY) S.st_heavy += k - nstale - nrepush;
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) dv[j] = ev[j] != 0xFFFFFFFFu ? __ldcg(Q.dist + ev[j]) : 0u;
+  unsigned nstale = 0, nrepush = 0, nheavy = 0;
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    const unsigned i = j * BLOCK + tid;
+    unsigned rb = 0, re = 0, du = 0;
+    const unsigned v = ev[j], d = ed[j];
+    if (v != 0xFFFFFFFFu) {
+      if (dv[j] != d) {
+        ++nstale; /* superseded: a later push carries the smaller value */
+      } else {
+        const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
+        if (b > d_base) { /* left in the far slot: move it to its own bucket */
+          stage<BLOCK, UU>(S, v, d, route(b, d_base));
+          ++nrepush;
+        } else {
+          const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
+          const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
+          if (mode == PH_M_LIGHT) {
+            rb = r0;
+            re = r0 + nl;
+            if (nl < r1 - r0) stage<BLOCK, UU>(S, v, d, PH_LSETTLED);
+          } else {
+            rb = r0 + nl;
+            re = r1;
+            ++nheavy;
+          }
+          if (re - rb > P.hub_threshold) { /* cut into chunks for the whole group */
+            const unsigned deg = re - rb;
+            const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
+            const unsigned hb = atomicAdd(&G->hub_count, nch);
+            if (hb + nch > P.hub_cap) {
+              raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
+            } else {
+              PhHub *hp = hub_of(P, c) + hb;
+              unsigned *sq = hub_seq_of(P, c) + hb;
+              for (unsigned x = 0; x < nch; ++x)
+                __stcg(reinterpret_cast<uint4 *>(hp + x),
+                       make_uint4(v, d, rb + x * P.hub_chunk,
+                                  rb + min(deg, (x + 1u) * P.hub_chunk)));
+              __threadfence(); /* the records before their sequence words */
+              const unsigned ep = S.D.epoch;
+              for (unsigned x = 0; x < nch; ++x) st_rlx32(sq + x, ep);
+            }
+            re = rb;
+          }
+          du = d;
+        }
+      }
+    }
+    S.it_rb[i] = rb;
+    S.it_du[i] = du;
+    S.it_off[i] = re - rb; /* the length, turned into an offset below */
+  }
+  /* statistics: one shared atomic per warp */
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nstale += __shfl_down_sync(0xFFFFFFFFu, nstale, o);
+    nrepush += __shfl_down_sync(0xFFFFFFFFu, nrepush, o);
+    nheavy += __shfl_down_sync(0xFFFFFFFFu, nheavy, o);
+  }
+  if ((tid & 31u) == 0u) {
+    if (nstale) atomicAdd(&S.st_stale, (unsigned long long)nstale);
+    if (nrepush) atomicAdd(&S.st_repush, (unsigned long long)nrepush);
+    if (nheavy) atomicAdd(&S.st_heavy, (unsigned long long)nheavy);
+  }
+  __syncthreads();
+  /* offsets in item order: thread t owns items [t*EPT, t*EPT + EPT) */
+  unsigned lens[EPT], mine = 0;
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    lens[j] = S.it_off[tid * EPT + j];
+    mine += lens[j];
   }
   unsigned tot;
-  const unsigned off = block_exscan<BLOCK, UU>(S, re - rb, tot);
-  S.it_off[tid] = off;
+  unsigned off = block_exscan<BLOCK, UU>(S, mine, tot);
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    S.it_off[tid * EPT + j] = off;
+    off += lens[j];
+  }
   if (tid == 0) {
-    S.it_off[BLOCK] = tot;
+    S.it_off[EPT * BLOCK] = tot;
     S.ck_k = k;
     S.ck_E = tot;
   }
@@ -870,7 +930,8 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     /* entries per claim: BLOCK, or fewer (a multiple of 32) so that a medium
      * frontier reaches every CTA of the group */
     const unsigned long long spread = (hi - lo + P.gsize - 1ull) / P.gsize;
-    S.D.per = (unsigned)min((unsigned long long)BLOCK, max(32ull, (spread + 31ull) & ~31ull));
+    S.D.per = (unsigned)min((unsigned long long)(PH_EPT * BLOCK),
+                            max(32ull, (spread + 31ull) & ~31ull));
   }
 }
 
@@ -964,7 +1025,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
         Waiter w{c.deadline, 0};
         bool ok = true;
         while (ld_acq32(&G->gen) == S.gen) {
-          if (!w.spin(P.g, W_BARRIER, 256)) {
+          if (!w.spin(P.g, W_BARRIER, 128)) {
             ok = false;
             break;
           }
@@ -1043,9 +1104,10 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
 }  // namespace adds_phase
 
 /* Kernel variants: (threads per CTA, CTAs per SM the registers are sized
- * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1 (64 registers per
- * thread), 3: 256 x 2, 4: 512 x 1 (128 registers per thread). */
-#define PH_VARIANTS(X) X(0, 256, 4) X(1, 512, 2) X(2, 1024, 1) X(3, 256, 2) X(4, 512, 1)
+ * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1, 5: 128 x 8 (64
+ * registers per thread), 3: 256 x 2, 4: 512 x 1 (128 registers per thread). */
+#define PH_VARIANTS(X) \
+  X(0, 256, 4) X(1, 512, 2) X(2, 1024, 1) X(3, 256, 2) X(4, 512, 1) X(5, 128, 8)
 
 int adds_phase_variant_block(int variant) {
 #define X(i, b, m) if (variant == i) return b;

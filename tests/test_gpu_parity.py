@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 OPTS = dict(timeout_ms=10000)
 ASYNC, PHASE = 1, 2
 # phase-engine kernel variants: (threads per CTA, CTAs per SM)
-VARIANTS = [(256, 4), (512, 2), (1024, 1), (256, 2), (512, 1)]
+VARIANTS = [(256, 4), (512, 2), (1024, 1), (256, 2), (512, 1), (128, 8)]
 
 
 def _check(g, src, **kw):
