@@ -1369,6 +1369,12 @@ extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs
   b->dist_off.resize(nq);
   b->shifts.resize(nq);
   b->scales.resize(nq);
+  /* launch-wide knobs (engine, kernel variant, group size...) come from the
+   * largest query's graph: the one worth tuning, and the one that dominates
+   * the launch; bucket widths stay per query */
+  uint32_t big = 0;
+  for (uint32_t i = 1; i < nq; ++i)
+    if ((uint64_t)graphs[i]->n + graphs[i]->m > (uint64_t)graphs[big]->n + graphs[big]->m) big = i;
   for (uint32_t i = 0; i < nq; ++i) {
     adds_graph *g = graphs[i];
     auto it = std::find(b->ugraph.begin(), b->ugraph.end(), g);
@@ -1379,7 +1385,7 @@ extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs
     tot += ((size_t)g->n + 31) & ~(size_t)31;
     Knobs k;
     resolve(g, opts, &k, &b->shifts[i], &b->scales[i]);
-    if (i == 0) b->kn = k;
+    if (i == big) b->kn = k;
   }
   if (cudaMalloc(&b->dist_all, tot * 4) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||

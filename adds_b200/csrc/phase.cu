@@ -1200,8 +1200,11 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
     E.gsize = nctas;
     E.groups = 1;
   } else {
+    /* about 32 groups: enough to run small queries side by side, large
+     * enough that a big query still has a few SMs (measured best on the
+     * mixed 256-query batch: 18 CTAs per group on 148 SMs) */
     unsigned gs = k.group_ctas > 0 ? (unsigned)k.group_ctas
-                                   : std::max(1u, nctas / std::min(E.nq, 64u));
+                                   : std::max(1u, nctas / std::min(E.nq, 32u));
     gs = std::min(gs, nctas);
     E.gsize = gs;
     E.groups = std::min(nctas / gs, E.nq);

@@ -416,7 +416,8 @@ def run_batched(args, ws, rank, local, dist):
     rsrc = [int(x) for x in rng.choice(cand, size=64, replace=False)]
     qg = graphs + [r20] * 64
     qs = srcs + rsrc
-    opts = A.default_opts(timeout_ms=60000)
+    opts = A.default_opts(timeout_ms=60000, engine=args.engine,
+                          **(json.loads(args.opts) if args.opts else {}))
     # the autotuner picks per-graph knobs on a representative member
     if not args.no_tune:
         r20.tune(rsrc[:2])
@@ -520,7 +521,8 @@ def run_diff(args, ws, rank, local, dist):
     if not args.no_tune:
         big = int(np.argmax(sides))
         graphs[big].tune([qs[qi.index(big)]])
-    b = A.Batch(qg, qs, A.default_opts(timeout_ms=60000))
+    b = A.Batch(qg, qs, A.default_opts(timeout_ms=60000, engine=args.engine,
+                                       **(json.loads(args.opts) if args.opts else {})))
     params = [th.clone().requires_grad_(True) for th in thetas]
     off = torch.from_numpy(b.layout()[0].astype(np.int64)).cuda()
     # flat indices of (query, target) pairs and their coefficients
