@@ -66,6 +66,42 @@ def test_phase_schedules_int_rmat(variant, solo, lh):
                block_threads=variant[0], ctas_per_sm=variant[1], hub_threshold=64)
 
 
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
+@pytest.mark.parametrize("wt", [G.I32, G.F32])
+def test_frontier_bellman_ford(engine, wt):
+    """delta_shift 31 with light/heavy off is frontier Bellman-Ford (every
+    distance in one bucket): the comparator the reference ran through nf/nv
+    (nf_int.patch, nv_int/kernel.cu), here as a schedule of the same engine."""
+    g = (G.rmat(13, 16, seed=14, w_hi=10000) if wt == G.I32 else
+         G.grid(120, 90, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=15))
+    _check(g, 0 if wt == G.F32 else G.max_degree_vertex(g), engine=engine, delta_shift=31,
+           light_heavy=0)
+
+
+def test_phase_trace_and_stats():
+    """The phase trace records every decided phase in time order and the
+    statistics account for the work (pops = stale + expanded)."""
+    g = G.rmat(14, 16, seed=16, w_hi=10000)
+    src = G.max_degree_vertex(g)
+    dg = A.Graph.from_csr(g)
+    try:
+        dg.trace(4096)
+        d, st = dg.sssp(src, A.default_opts(**OPTS, engine=PHASE, delta_shift=8, solo_max=64))
+        tr, n = dg.trace_read(4096)
+        dg.trace(0)
+    finally:
+        dg.close()
+    ref, _ = O.dijkstra(g, src)
+    assert np.array_equal(d, ref)
+    assert n == len(tr) and n == st["phases"]  # one record per decision, exit included
+    assert (np.diff(tr["t_ns"].astype(np.int64)) >= 0).all()
+    modes = tr["mode"] & 0xFF
+    assert modes[0] == 0 and modes[-1] == 4  # init first, exit last
+    assert ((tr["mode"] & 0x100) != 0).sum() == st["solo_phases"]
+    assert st["items_popped"] >= st["items_stale"] and st["edges_scanned"] > 0
+    assert st["engine"] == PHASE and st["ctas"] > 0
+
+
 @pytest.mark.parametrize("variant", VARIANTS[:3])
 @pytest.mark.parametrize("lh", [0, 1])
 def test_phase_schedules_float_grid(variant, lh):
