@@ -362,6 +362,101 @@ __device__ __forceinline__ unsigned block_exscan(PSmem<BLOCK, UU> &S, unsigned x
  * thread walks its share of the chunk's edges with no barrier until the
  * chunk is done.                                                             */
 
+/* Items from one entry (v, d) of a light or heavy phase: the stale check,
+ * the far-slot re-push, the light / heavy row segment, the settled push and
+ * the split of long rows into records.  Returns the segment in rb/re (empty
+ * when nothing is to be expanded) and counts what it did. */
+template <bool FLT, int BLOCK, int UU>
+__device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S,
+                                           const PhQuery &Q, unsigned v, unsigned d, unsigned dv,
+                                           unsigned &rb, unsigned &re, unsigned &du,
+                                           unsigned &nstale, unsigned &nrepush, unsigned &nheavy) {
+  PhGroup *G = grp_of(P, c);
+  const unsigned mode = S.D.mode, d_base = S.D.base;
+  rb = re = du = 0u;
+  if (dv != d) {
+    ++nstale; /* superseded: a later push carries the smaller value */
+    return;
+  }
+  const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
+  if (b > d_base) { /* left in the far slot: move it to its own bucket */
+    stage<BLOCK, UU>(S, v, d, route(b, d_base));
+    ++nrepush;
+    return;
+  }
+  const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
+  const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
+  if (mode == PH_M_LIGHT) {
+    rb = r0;
+    re = r0 + nl;
+    if (nl < r1 - r0) stage<BLOCK, UU>(S, v, d, PH_LSETTLED);
+  } else {
+    rb = r0 + nl;
+    re = r1;
+    ++nheavy;
+  }
+  if (re - rb > P.hub_threshold) { /* cut into chunks for the whole group */
+    const unsigned deg = re - rb;
+    const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
+    const unsigned hb = atomicAdd(&G->hub_count, nch);
+    if (hb + nch > P.hub_cap) {
+      raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
+    } else {
+      PhHub *hp = hub_of(P, c) + hb;
+      unsigned *sq = hub_seq_of(P, c) + hb;
+      for (unsigned x = 0; x < nch; ++x)
+        __stcg(reinterpret_cast<uint4 *>(hp + x),
+               make_uint4(v, d, rb + x * P.hub_chunk, rb + min(deg, (x + 1u) * P.hub_chunk)));
+      __threadfence(); /* the records before their sequence words */
+      const unsigned ep = S.D.epoch;
+      for (unsigned x = 0; x < nch; ++x) st_rlx32(sq + x, ep);
+    }
+    re = rb;
+  }
+  du = d;
+}
+
+/* Finishes a chunk whose items' lengths are in it_off: statistics, the
+ * exclusive scan of the lengths, the chunk totals. */
+template <int BLOCK, int UU>
+__device__ __forceinline__ void finish_items(PSmem<BLOCK, UU> &S, unsigned k, unsigned nstale,
+                                             unsigned nrepush, unsigned nheavy) {
+  constexpr int EPT = PSmem<BLOCK, UU>::EPT;
+  const unsigned tid = threadIdx.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nstale += __shfl_down_sync(0xFFFFFFFFu, nstale, o);
+    nrepush += __shfl_down_sync(0xFFFFFFFFu, nrepush, o);
+    nheavy += __shfl_down_sync(0xFFFFFFFFu, nheavy, o);
+  }
+  if ((tid & 31u) == 0u) {
+    if (nstale) atomicAdd(&S.st_stale, (unsigned long long)nstale);
+    if (nrepush) atomicAdd(&S.st_repush, (unsigned long long)nrepush);
+    if (nheavy) atomicAdd(&S.st_heavy, (unsigned long long)nheavy);
+  }
+  __syncthreads();
+  /* offsets in item order: thread t owns items [t*EPT, t*EPT + EPT) */
+  unsigned lens[EPT], mine = 0;
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    lens[j] = S.it_off[tid * EPT + j];
+    mine += lens[j];
+  }
+  unsigned tot;
+  unsigned off = block_exscan<BLOCK, UU>(S, mine, tot);
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    S.it_off[tid * EPT + j] = off;
+    off += lens[j];
+  }
+  if (tid == 0) {
+    S.it_off[EPT * BLOCK] = tot;
+    S.ck_k = k;
+    S.ck_E = tot;
+  }
+  __syncthreads();
+}
+
 /* Claims and prepares the next chunk.  Returns false when the phase has no
  * more chunks.  Every thread calls it. */
 template <bool FLT, int BLOCK, int UU>
@@ -449,87 +544,14 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
   for (int j = 0; j < EPT; ++j) {
     const unsigned i = j * BLOCK + tid;
     unsigned rb = 0, re = 0, du = 0;
-    const unsigned v = ev[j], d = ed[j];
-    if (v != 0xFFFFFFFFu) {
-      if (dv[j] != d) {
-        ++nstale; /* superseded: a later push carries the smaller value */
-      } else {
-        const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
-        if (b > d_base) { /* left in the far slot: move it to its own bucket */
-          stage<BLOCK, UU>(S, v, d, route(b, d_base));
-          ++nrepush;
-        } else {
-          const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
-          const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
-          if (mode == PH_M_LIGHT) {
-            rb = r0;
-            re = r0 + nl;
-            if (nl < r1 - r0) stage<BLOCK, UU>(S, v, d, PH_LSETTLED);
-          } else {
-            rb = r0 + nl;
-            re = r1;
-            ++nheavy;
-          }
-          if (re - rb > P.hub_threshold) { /* cut into chunks for the whole group */
-            const unsigned deg = re - rb;
-            const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
-            const unsigned hb = atomicAdd(&G->hub_count, nch);
-            if (hb + nch > P.hub_cap) {
-              raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
-            } else {
-              PhHub *hp = hub_of(P, c) + hb;
-              unsigned *sq = hub_seq_of(P, c) + hb;
-              for (unsigned x = 0; x < nch; ++x)
-                __stcg(reinterpret_cast<uint4 *>(hp + x),
-                       make_uint4(v, d, rb + x * P.hub_chunk,
-                                  rb + min(deg, (x + 1u) * P.hub_chunk)));
-              __threadfence(); /* the records before their sequence words */
-              const unsigned ep = S.D.epoch;
-              for (unsigned x = 0; x < nch; ++x) st_rlx32(sq + x, ep);
-            }
-            re = rb;
-          }
-          du = d;
-        }
-      }
-    }
+    if (ev[j] != 0xFFFFFFFFu)
+      entry_item<FLT, BLOCK, UU>(P, c, S, Q, ev[j], ed[j], dv[j], rb, re, du, nstale, nrepush,
+                                 nheavy);
     S.it_rb[i] = rb;
     S.it_du[i] = du;
     S.it_off[i] = re - rb; /* the length, turned into an offset below */
   }
-  /* statistics: one shared atomic per warp */
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    nstale += __shfl_down_sync(0xFFFFFFFFu, nstale, o);
-    nrepush += __shfl_down_sync(0xFFFFFFFFu, nrepush, o);
-    nheavy += __shfl_down_sync(0xFFFFFFFFu, nheavy, o);
-  }
-  if ((tid & 31u) == 0u) {
-    if (nstale) atomicAdd(&S.st_stale, (unsigned long long)nstale);
-    if (nrepush) atomicAdd(&S.st_repush, (unsigned long long)nrepush);
-    if (nheavy) atomicAdd(&S.st_heavy, (unsigned long long)nheavy);
-  }
-  __syncthreads();
-  /* offsets in item order: thread t owns items [t*EPT, t*EPT + EPT) */
-  unsigned lens[EPT], mine = 0;
-#pragma unroll
-  for (int j = 0; j < EPT; ++j) {
-    lens[j] = S.it_off[tid * EPT + j];
-    mine += lens[j];
-  }
-  unsigned tot;
-  unsigned off = block_exscan<BLOCK, UU>(S, mine, tot);
-#pragma unroll
-  for (int j = 0; j < EPT; ++j) {
-    S.it_off[tid * EPT + j] = off;
-    off += lens[j];
-  }
-  if (tid == 0) {
-    S.it_off[EPT * BLOCK] = tot;
-    S.ck_k = k;
-    S.ck_E = tot;
-  }
-  __syncthreads();
+  finish_items<BLOCK, UU>(S, k, nstale, nrepush, nheavy);
   return true;
 }
 
@@ -749,6 +771,7 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
     }
     if (!have) {
       if (records) break;
+
       /* no frontier chunk left for this CTA: it appends no more split rows,
        * and helps expand the ones the group has appended */
       records = true;

@@ -126,7 +126,6 @@ struct __align__(128) PhGlobal {
                                    leader (solo phases included), grid-phase
                                    work, total                                */
   unsigned long long st_trace;  /* trace records written (may exceed the cap) */
-  unsigned long long st_direct; /* pushes that bypassed a full staging buffer */
 };
 
 /* One record of the phase trace (group 0 only): when the leader decided a
