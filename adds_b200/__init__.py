@@ -151,6 +151,13 @@ class Graph:
         check(lib().adds_graph_reached(self._h, C.byref(r), C.byref(e)), "adds_graph_reached")
         return r.value, e.value
 
+    def relax_ceiling(self, src: int):
+        """Times one pass over every edge with the final distances from src:
+        stream only, gather, gather + reduction, reduction only (ms)."""
+        out = (C.c_double * 4)()
+        check(lib().adds_diag_relax_pass(self._h, src, out), "adds_diag_relax_pass")
+        return list(out)
+
     def trace(self, cap: int) -> None:
         """Records up to cap phases of each later solve (0 turns it off)."""
         check(lib().adds_graph_trace(self._h, cap), "adds_graph_trace")

@@ -30,7 +30,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-Wall", "-I", os.path.join(ROOT, "include")]
-CU_SOURCES = ["engine.cu", "phase.cu", "api.cu", "gen.cu", "adjoint.cu", "noalloc.cu"]
+CU_SOURCES = ["engine.cu", "phase.cu", "api.cu", "gen.cu", "adjoint.cu", "noalloc.cu", "diag.cu"]
 CXX_SOURCES = ["grio.cpp"]
 
 

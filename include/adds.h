@@ -290,6 +290,16 @@ int adds_graph_trace(adds_graph *g, uint32_t cap);
 int adds_graph_trace_read(adds_graph *g, adds_phase_trace *out, uint32_t cap,
                           uint64_t *written);
 
+/* ---- relaxation ceiling (diagnostics) ----------------------------------- */
+/* No counterpart in the reference.  Solves from src, then times one pass over
+ * every edge of g with those final distances resident, four ways: ms_out[0]
+ * streaming each edge and its source's distance (12 B per edge), [1] the same
+ * plus the random gather of dist[dst] and the comparison, [2] plus a
+ * min-reduction where the comparison succeeds, [3] a min-reduction on every
+ * edge without the gather.  [1] bounds any push-based relaxation schedule on
+ * this GPU.  Allocates (the pass needs 4 B per edge and two distance arrays). */
+int adds_diag_relax_pass(adds_graph *g, uint32_t src, double ms_out[4]);
+
 /* ---- autotuner ---------------------------------------------------------- */
 /* Times candidate settings on the sample sources and stores the fastest in
  * the graph (used whenever a later call passes "auto" knobs): delta, then for

@@ -211,3 +211,15 @@ def test_engine_matches_reference_adds_output(name):
         assert np.array_equal(d, z["dist"])
     else:
         assert G.dist_text(d, G.F32) == gzip.decompress(z["text_gz"].tobytes()).decode()
+
+
+def test_relax_ceiling_diagnostic():
+    """adds_diag_relax_pass: four positive pass times; the pass with the
+    gather is not faster than the pure stream."""
+    g = G.rmat(15, 16, seed=17, w_hi=10000)
+    dg = A.Graph.from_csr(g)
+    try:
+        ms = dg.relax_ceiling(G.max_degree_vertex(g))
+    finally:
+        dg.close()
+    assert len(ms) == 4 and all(x > 0 for x in ms)
