@@ -469,7 +469,9 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
   const unsigned long long d_lo = S.D.lo, d_hi = S.D.hi, d_wb = S.D.work_base;
   const unsigned d_base = S.D.base, d_list = S.D.list;
   constexpr unsigned IC = PSmem<BLOCK, UU>::IC;
-  const unsigned long long count = d_hi - d_lo;
+  const unsigned nx = mode == PH_M_LIGHT ? S.D.nx : 0u; /* ranges past the first */
+  unsigned long long count = d_hi - d_lo;
+  for (unsigned r = 0; r < nx; ++r) count += S.D.xhi[r] - S.D.xlo[r];
   __syncthreads(); /* everyone has read the previous claim's S.stop */
   if (tid == 0) {
     /* guided self-scheduling: a claim takes about half this CTA's share of
@@ -501,7 +503,11 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
     }
     S.claim = at;
     S.stop = at >= count ? 1u : 0u;
-    if (!S.stop) {
+    if (!S.stop && nx != 0u) { /* a widened bucket: each thread maps its entry */
+      S.ck_k = (unsigned)min((unsigned long long)n, count - at);
+      ++S.st_chunks;
+      S.st_items += S.ck_k;
+    } else if (!S.stop) {
       const unsigned long long s0 = d_lo + at;
       const unsigned long long s1 = min(s0 + n, d_hi) - 1ull;
       S.ck_k = (unsigned)(s1 + 1ull - s0);
@@ -527,7 +533,22 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
     const unsigned i = j * BLOCK + tid;
     ev[j] = 0xFFFFFFFFu;
     ed[j] = 0u;
-    if (i < k) {
+    if (i < k && nx != 0u) { /* find the entry's range, then its page */
+      unsigned long long pos = S.claim + i, span = d_hi - d_lo, idx = d_lo + pos;
+      unsigned L = d_list;
+      for (unsigned r = 0; r < nx && pos >= span; ++r) {
+        pos -= span;
+        L = S.D.xl[r];
+        idx = S.D.xlo[r] + pos;
+        span = S.D.xhi[r] - S.D.xlo[r];
+      }
+      const unsigned pg = pt_lookup(P, c, L, idx >> PH_PAGE_LOG2);
+      if (pg != 0xFFFFFFFFu) {
+        const unsigned long long e = __ldcg(entry_ptr(P, c, pg, idx));
+        ev[j] = (unsigned)e;
+        ed[j] = (unsigned)(e >> 32);
+      }
+    } else if (i < k) {
       const unsigned long long idx = s0 + i;
       const unsigned pg = ((idx >> PH_PAGE_LOG2) == (s0 >> PH_PAGE_LOG2)) ? S.pi0 : S.pi1;
       if (pg != 0xFFFFFFFFu) {
@@ -818,6 +839,8 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   bool hub_only = false;
   unsigned mode = PH_M_EXIT, q = prev_q, list = 0, base = ld_rlx32(&G->base);
   unsigned long long lo = 0, hi = 0;
+  unsigned nx = 0, xl[PH_MAXR - 1] = {0u, 0u, 0u};
+  unsigned long long xlo[PH_MAXR - 1] = {0ull, 0ull, 0ull}, xhi[PH_MAXR - 1] = {0ull, 0ull, 0ull};
   bool decide = false, next_query = false;
   if (ld_rlx32(&P.g->err) != 0u) {
     mode = PH_M_EXIT;
@@ -879,13 +902,41 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       const unsigned ma = __ballot_sync(0xFFFFFFFFu, ta > ha);
       const unsigned mb = __ballot_sync(0xFFFFFFFFu, offb < PH_NSLOT && tb > hb);
       if (ma | mb) {
-        const unsigned off = ma ? (unsigned)__ffs(ma) : 32u + (unsigned)__ffs(mb);
-        const unsigned sl = (base + off) & (PH_NSLOT - 1u);
+        /* the nearest non-empty slot; with adaptation on, while the entries
+         * gathered stay few, the next non-empty slots too (at most PH_MAXR,
+         * never the far slot after another): the bucket is widened on the
+         * device and the ring re-based at the window's top bucket.  Relaxing
+         * a wider bucket is still label-correcting: a distance that a later
+         * heavy phase lowers to the window comes back through the NEXT list */
+        unsigned long long mask = (unsigned long long)ma | ((unsigned long long)mb << 32);
+        const unsigned long long target =
+            max(4ull * P.solo_max, 32ull * P.gsize);
+        unsigned long long cum = 0;
+        unsigned top = 0;
+        while (mask != 0ull) {
+          const unsigned i = (unsigned)__ffsll((long long)mask) - 1u;
+          const unsigned off = i + 1u;
+          if (off == PH_NSLOT - 1u && top != 0u) break;
+          const unsigned long long t = __shfl_sync(0xFFFFFFFFu, i < 32u ? ta : tb, i & 31u);
+          const unsigned long long h = __shfl_sync(0xFFFFFFFFu, i < 32u ? ha : hb, i & 31u);
+          const unsigned sl = (base + off) & (PH_NSLOT - 1u);
+          if (top == 0u) {
+            list = sl;
+            lo = h;
+            hi = t;
+          } else {
+            xl[nx] = sl;
+            xlo[nx] = h;
+            xhi[nx] = t;
+            ++nx;
+          }
+          top = off;
+          cum += t - h;
+          mask &= mask - 1ull;
+          if (!P.adapt || cum >= target || nx + 1u == PH_MAXR || off == PH_NSLOT - 1u) break;
+        }
         mode = PH_M_LIGHT;
-        list = sl;
-        base += off;
-        lo = ld_rlx64(&G->head[sl]);
-        hi = ld_rlx64(&G->tails[sl].tail);
+        base += top;
         if (lane == 0) st_rlx32(&G->base, base);
       } else {
         next_query = true;
@@ -893,6 +944,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     }
     if ((mode == PH_M_LIGHT || mode == PH_M_HEAVY) && lane == 0) {
       st_rlx64(&G->head[list], hi);
+      for (unsigned r = 0; r < nx; ++r) st_rlx64(&G->head[xl[r]], xhi[r]);
       st_rlx32(&G->hub_count, 0u); /* split rows of the coming phase */
       st_rlx32(&G->hub_claim, 0u);
     }
@@ -930,12 +982,14 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     st_rlx32(&G->epoch, epoch);
   }
   __syncwarp();
+  unsigned long long total = hi - lo;
+  for (unsigned r = 0; r < nx; ++r) total += xhi[r] - xlo[r];
   if (lane == 0 && P.trace && c.gi == 0u) {
     const unsigned long long i = atomicAdd(&P.g->st_trace, 1ull);
     if (i < P.trace_cap) {
       PhTrace tr;
       tr.t_ns = gtimer();
-      tr.count = mode == PH_M_INIT ? P.qs[q].n : (unsigned)min(hi - lo, 0xFFFFFFFFull);
+      tr.count = mode == PH_M_INIT ? P.qs[q].n : (unsigned)min(total, 0xFFFFFFFFull);
       tr.mode = (unsigned short)mode;
       tr.base = (unsigned short)base;
       P.trace[i] = tr;
@@ -950,9 +1004,15 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     S.D.hi = hi;
     S.D.work_base = wb;
     S.D.epoch = epoch;
+    S.D.nx = nx;
+    for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
+      S.D.xl[r] = xl[r];
+      S.D.xlo[r] = xlo[r];
+      S.D.xhi[r] = xhi[r];
+    }
     /* entries per claim: BLOCK, or fewer (a multiple of 32) so that a medium
      * frontier reaches every CTA of the group */
-    const unsigned long long spread = (hi - lo + P.gsize - 1ull) / P.gsize;
+    const unsigned long long spread = (total + P.gsize - 1ull) / P.gsize;
     S.D.per = (unsigned)min((unsigned long long)(PH_EPT * BLOCK),
                             max(32ull, (spread + 31ull) & ~31ull));
   }
@@ -962,7 +1022,11 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
 template <int BLOCK, int UU>
 __device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK, UU> &S) {
   const unsigned mode = S.D.mode;
-  if (mode == PH_M_LIGHT || mode == PH_M_HEAVY) return S.D.hi - S.D.lo <= P.solo_max;
+  if (mode == PH_M_LIGHT || mode == PH_M_HEAVY) {
+    unsigned long long total = S.D.hi - S.D.lo;
+    for (unsigned r = 0; r < S.D.nx; ++r) total += S.D.xhi[r] - S.D.xlo[r];
+    return total <= P.solo_max;
+  }
   if (mode == PH_M_HUB) return false; /* left by a solo phase because it is large */
   if (mode == PH_M_INIT) return P.qs[S.D.q].n <= 64u * BLOCK;
   return false;
@@ -1064,6 +1128,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
           S.D.work_base = ld_rlx64(&dp->work_base);
           S.D.per = ld_rlx32(&dp->per);
           S.D.epoch = ld_rlx32(&dp->epoch);
+          S.D.nx = ld_rlx32(&dp->nx);
+          for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
+            S.D.xl[r] = ld_rlx32(&dp->xl[r]);
+            S.D.xlo[r] = ld_rlx64(&dp->xlo[r]);
+            S.D.xhi[r] = ld_rlx64(&dp->xhi[r]);
+          }
         } else {
           S.D.mode = PH_M_EXIT;
         }
@@ -1314,6 +1384,7 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->hub_chunk = ph_hub_chunk(k);
   if (P->hub_chunk < E.hub_eff) return -9; /* engine sized for longer chunks */
   P->solo_max = k.solo_max;
+  P->adapt = k.adapt;
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

@@ -65,6 +65,7 @@ struct __align__(16) PhHub {
 
 /* What every CTA of a group needs for one phase (written by the leader before
  * it releases the barrier; double-buffered by barrier generation). */
+#define PH_MAXR 4 /* list ranges one light phase may read (widened bucket) */
 struct __align__(64) PhDesc {
   unsigned mode;
   unsigned q;                  /* query index                                */
@@ -74,6 +75,11 @@ struct __align__(64) PhDesc {
   unsigned long long work_base; /* claim counter value at phase start        */
   unsigned per;                /* entries per claim                           */
   unsigned epoch;              /* phase number: marks its split-row records    */
+  /* a light phase whose bucket the leader widened over thin slots reads
+   * nx further ranges after (list, lo, hi) */
+  unsigned nx;
+  unsigned xl[PH_MAXR - 1];
+  unsigned long long xlo[PH_MAXR - 1], xhi[PH_MAXR - 1];
   unsigned pad[4];
 };
 
@@ -156,6 +162,7 @@ struct PhParams {
   unsigned hub_threshold;      /* rows with more expanded edges are split     */
   unsigned hub_chunk;          /* edges per split chunk                       */
   unsigned solo_max;           /* frontiers up to this size run on the leader */
+  unsigned adapt;              /* merge thin bucket slots into one phase      */
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
@@ -194,7 +201,7 @@ struct PhKnobs {
   int variant;        /* kernel variant (threads x CTAs per SM), phase.cu      */
   int ctas_per_sm;    /* <= 0: as many as fit                                 */
   int group_ctas;     /* CTAs per group (batches); <= 0: automatic            */
-  unsigned hub_threshold, hub_chunk, solo_max;
+  unsigned hub_threshold, hub_chunk, solo_max, adapt;
   unsigned long long timeout_ns;
 };
 

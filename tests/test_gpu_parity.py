@@ -111,6 +111,50 @@ def test_phase_schedules_float_grid(variant, lh):
                block_threads=variant[0], ctas_per_sm=variant[1], solo_max=256)
 
 
+@pytest.mark.parametrize("adapt", [0, 1])
+@pytest.mark.parametrize("solo", [0, 64])
+@pytest.mark.parametrize("lh", [0, 1])
+def test_phase_bucket_widening(adapt, solo, lh):
+    """The leader widens a bucket over up to four thin consecutive slots
+    (adapt 1): the distances stay the oracle's, int32 and float32, with the
+    far slot in use (shift 2 on the R-MAT, shift 8 on the grid)."""
+    g = G.rmat(12, 16, seed=21, w_hi=10000)
+    for shift in (2, 7, 11):
+        _check(g, G.max_degree_vertex(g), engine=PHASE, delta_shift=shift, light_heavy=lh,
+               solo_max=solo, adapt=adapt, hub_threshold=64)
+    g = G.grid(150, 100, 0.02, 8, wtype=G.F32, w_lo=0.0, w_hi=3.0, seed=22)
+    for shift in (8, 14):
+        _check(g, 75, engine=PHASE, delta_shift=shift, light_heavy=lh, solo_max=solo,
+               adapt=adapt)
+
+
+def test_phase_bucket_widening_merges_thin_slots():
+    """On a high-diameter grid with a narrow bucket, widening takes fewer
+    phases than one bucket slot per phase, and the trace shows the base
+    advancing by more than one bucket in a single light phase."""
+    g = G.grid(160, 120, 0.0, 8, wtype=G.F32, w_lo=1.0, w_hi=2.0, seed=23)
+    dg = A.Graph.from_csr(g)
+    try:
+        res = {}
+        for adapt in (0, 1):
+            dg.trace(1 << 16)
+            d, st = dg.sssp(0, A.default_opts(**OPTS, engine=PHASE, delta_shift=14,
+                                              solo_max=4096, adapt=adapt))
+            tr, n = dg.trace_read(1 << 16)
+            dg.trace(0)
+            res[adapt] = (d, st, tr)
+    finally:
+        dg.close()
+    ref, _ = O.dijkstra(g, 0)
+    for adapt in (0, 1):
+        assert np.array_equal(res[adapt][0], ref)
+    assert res[1][1]["phases"] < res[0][1]["phases"]
+    tr = res[1][2]
+    light = (tr["mode"] & 0xFF) == 1
+    steps = np.diff(tr["base"].astype(np.int64))[light[1:]]
+    assert (steps > 1).any()
+
+
 def test_phase_float_grid_large_keys():
     """A high-diameter float grid with a narrow bucket (many slots, far-slot
     re-pushes) and zero-weight edges mixed in."""
