@@ -164,9 +164,12 @@ class Graph:
 
     def trace_read(self, cap: int = 1 << 16):
         """The last solve's phase records as a numpy structured array
-        (t_ns, count, mode, base) and the number the solve produced."""
+        (t_ns, count, mode, base, edges, items, pushes, tail_ns) and the
+        number the solve produced."""
         import numpy as np
-        dt = np.dtype([("t_ns", "<u8"), ("count", "<u4"), ("mode", "<u2"), ("base", "<u2")])
+        dt = np.dtype([("t_ns", "<u8"), ("count", "<u4"), ("mode", "<u2"), ("base", "<u2"),
+                       ("edges", "<u4"), ("items", "<u4"), ("pushes", "<u4"),
+                       ("tail_ns", "<u4")])
         buf = np.zeros(cap, dtype=dt)
         n = C.c_uint64()
         check(lib().adds_graph_trace_read(self._h, buf.ctypes.data, cap, C.byref(n)),

@@ -288,6 +288,7 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.hub_chunk = 1024u;
   p.solo_max = (unsigned)std::max(0, k.solo_max);
   p.adapt = k.adapt > 0 ? 1u : 0u;
+  p.lh_adapt = k.light_heavy == 2 ? 1u : 0u;
   p.timeout_ns = k.timeout_ns;
   return p;
 }
@@ -832,11 +833,15 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
 
   k->strict = o->strict_order >= 0 ? o->strict_order : (t->strict_order >= 0 ? t->strict_order : 1);
   k->local_max = o->local_max >= 0 ? o->local_max : (t->local_max >= 0 ? t->local_max : 512);
-  k->light_heavy = o->light_heavy >= 0 ? o->light_heavy : (t->light_heavy >= 0 ? t->light_heavy : 1);
   k->block = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 256);
   k->greed = o->greed >= 0 ? o->greed : (t->greed >= 0 ? t->greed : 4);
   k->engine = o->engine > 0 ? o->engine : (t->engine > 0 ? t->engine : ADDS_ENGINE_PHASE);
   if (k->engine != ADDS_ENGINE_ASYNC) k->engine = ADDS_ENGINE_PHASE;
+  /* light/heavy split: adaptive (2) in the phase engine, always (1) in the
+   * asynchronous one, which treats 2 as 1 */
+  k->light_heavy = o->light_heavy >= 0 ? o->light_heavy
+                                       : (t->light_heavy >= 0 ? t->light_heavy
+                                                              : (k->engine == ADDS_ENGINE_PHASE ? 2 : 1));
   /* on-device bucket widening (phase engine): off unless asked or tuned */
   k->adapt = o->adapt >= 0 ? o->adapt : (t->adapt >= 0 ? t->adapt : 0);
   const int hub_def = k->engine == ADDS_ENGINE_PHASE ? 256 : 16384;
@@ -1719,7 +1724,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
     }
     try_field(&adds_opts::solo_max, {0, 256, 512, 1024, 2048, 4096});
     try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
-    try_field(&adds_opts::light_heavy, {0, 1});
+    try_field(&adds_opts::light_heavy, {0, 1, 2});
     try_field(&adds_opts::adapt, {0, 1});
     if (cur.delta_shift != s0) {
       std::vector<int> s2;

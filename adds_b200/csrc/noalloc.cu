@@ -205,6 +205,7 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   P.hub_chunk = kHubThreshold;
   P.solo_max = 1024;
   P.adapt = 0u;
+  P.lh_adapt = 1u;
   P.is_float = flt ? 1u : 0u;
   P.single_src = 0xFFFFFFFFu;
   P.timeout_ns = 20000ull * 1000000ull;

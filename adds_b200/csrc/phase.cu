@@ -163,6 +163,7 @@ struct PSmem {
                                waits), expand, flush, barrier wait, leader,
                                grid-phase work, total */
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
+  unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
 };
 
 /* what a CTA keeps for the kernel's lifetime; the group's arrays are
@@ -171,6 +172,7 @@ struct Ctx {
   unsigned gi, rank;
   unsigned long long deadline;
   unsigned edges; /* per-thread count; the rest is counted in shared memory */
+  unsigned edges_mark; /* trace: c.edges at the end of the last phase         */
 };
 __device__ __forceinline__ PhGroup *grp_of(const PhParams &P, const Ctx &c) { return P.grp + c.gi; }
 
@@ -385,7 +387,7 @@ __device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOC
     return;
   }
   const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
-  const unsigned nl = Q.split ? __ldg(Q.split + v) : (r1 - r0);
+  const unsigned nl = (Q.split && !S.D.full) ? __ldg(Q.split + v) : (r1 - r0);
   if (mode == PH_M_LIGHT) {
     rb = r0;
     re = r0 + nl;
@@ -839,7 +841,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   bool hub_only = false;
   unsigned mode = PH_M_EXIT, q = prev_q, list = 0, base = ld_rlx32(&G->base);
   unsigned long long lo = 0, hi = 0;
-  unsigned nx = 0, xl[PH_MAXR - 1] = {0u, 0u, 0u};
+  unsigned nx = 0, xl[PH_MAXR - 1] = {0u, 0u, 0u}, full = 0u;
   unsigned long long xlo[PH_MAXR - 1] = {0ull, 0ull, 0ull}, xhi[PH_MAXR - 1] = {0ull, 0ull, 0ull};
   bool decide = false, next_query = false;
   if (ld_rlx32(&P.g->err) != 0u) {
@@ -857,6 +859,10 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       if (list_reserve(P, c, PH_LNEXT, 1u, &b, pg, &cvp, &cpi))
         st_rlx64(entry_ptr(P, c, pg[0], b), (unsigned long long)src);
       st_rlx32(&G->base, 0u);
+      /* the source's bucket counts as dense: it starts with split rows */
+      st_rlx32(&G->lh_dense, 1u);
+      st_rlx32(&G->lh_k, 0u);
+      st_rlx64(&G->lh_prev, 0ull);
       __threadfence();
     }
     __syncwarp();
@@ -883,6 +889,21 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       list = PH_LNEXT;
       lo = hn;
       hi = tn;
+      if (P.lh_adapt) {
+        /* another light phase of the same bucket: when it re-improved few of
+         * the vertices the last one expanded (under 1 in 20), heavy edges go
+         * with the light ones, and a bucket whose second light phase is that
+         * small marks the next bucket as sparse */
+        const unsigned long long prevc = ld_rlx64(&G->lh_prev);
+        const bool few = (tn - hn) * 20ull < prevc;
+        const unsigned k = ld_rlx32(&G->lh_k);
+        full = few ? 1u : 0u;
+        if (lane == 0) {
+          if (k == 1u && !few) st_rlx32(&G->lh_dense, 1u);
+          st_rlx64(&G->lh_prev, tn - hn);
+          st_rlx32(&G->lh_k, k + 1u);
+        }
+      }
     } else if (ts > hs) {
       mode = PH_M_HEAVY;
       list = PH_LSETTLED;
@@ -938,6 +959,15 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         mode = PH_M_LIGHT;
         base += top;
         if (lane == 0) st_rlx32(&G->base, base);
+        if (P.lh_adapt) {
+          /* a new bucket: whole rows unless the last bucket was dense */
+          full = ld_rlx32(&G->lh_dense) != 0u ? 0u : 1u;
+          if (lane == 0) {
+            st_rlx32(&G->lh_dense, 0u);
+            st_rlx64(&G->lh_prev, cum);
+            st_rlx32(&G->lh_k, 1u);
+          }
+        }
       } else {
         next_query = true;
       }
@@ -985,13 +1015,29 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   unsigned long long total = hi - lo;
   for (unsigned r = 0; r < nx; ++r) total += xhi[r] - xlo[r];
   if (lane == 0 && P.trace && c.gi == 0u) {
+    /* the phase that just ended: its work, and its barrier tail */
+    const unsigned long long now = gtimer();
+    const unsigned long long prev = ld_rlx64(&P.g->st_trace);
+    if (prev > 0ull && prev - 1ull < P.trace_cap) {
+      PhTrace *t = P.trace + (prev - 1ull);
+      const unsigned long long f = ld_rlx64(&G->tr_first);
+      t->edges = (unsigned)min(ld_rlx64(&G->tr_edges), 0xFFFFFFFFull);
+      t->items = (unsigned)min(ld_rlx64(&G->tr_items), 0xFFFFFFFFull);
+      t->pushes = (unsigned)min(ld_rlx64(&G->tr_pushes), 0xFFFFFFFFull);
+      t->tail_ns = (f != 0ull && now > f) ? (unsigned)min(now - f, 0xFFFFFFFFull) : 0u;
+    }
+    st_rlx64(&G->tr_first, 0ull);
+    st_rlx64(&G->tr_edges, 0ull);
+    st_rlx64(&G->tr_items, 0ull);
+    st_rlx64(&G->tr_pushes, 0ull);
     const unsigned long long i = atomicAdd(&P.g->st_trace, 1ull);
     if (i < P.trace_cap) {
       PhTrace tr;
-      tr.t_ns = gtimer();
+      tr.t_ns = now;
       tr.count = mode == PH_M_INIT ? P.qs[q].n : (unsigned)min(total, 0xFFFFFFFFull);
       tr.mode = (unsigned short)mode;
       tr.base = (unsigned short)base;
+      tr.edges = tr.items = tr.pushes = tr.tail_ns = 0u;
       P.trace[i] = tr;
     }
   }
@@ -1005,6 +1051,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     S.D.work_base = wb;
     S.D.epoch = epoch;
     S.D.nx = nx;
+    S.D.full = full;
     for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
       S.D.xl[r] = xl[r];
       S.D.xlo[r] = xlo[r];
@@ -1015,6 +1062,28 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     const unsigned long long spread = (total + P.gsize - 1ull) / P.gsize;
     S.D.per = (unsigned)min((unsigned long long)(PH_EPT * BLOCK),
                             max(32ull, (spread + 31ull) & ~31ull));
+  }
+}
+
+/* Trace of group 0: adds this CTA's work in the phase that just ended to the
+ * group's counters (every thread calls it). */
+template <int BLOCK, int UU>
+__device__ void trace_account(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
+  unsigned e = c.edges - c.edges_mark;
+  c.edges_mark = c.edges;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xFFFFFFFFu, e, o);
+  if ((threadIdx.x & 31u) == 0u && e != 0u) atomicAdd(&S.tr_e, (unsigned long long)e);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    PhGroup *G = grp_of(P, c);
+    const unsigned long long it = S.st_items + S.st_hubs, pu = S.st_pushes;
+    atomicAdd(&G->tr_edges, S.tr_e);
+    atomicAdd(&G->tr_items, it - S.tr_mi);
+    atomicAdd(&G->tr_pushes, pu - S.tr_mp);
+    S.tr_e = 0ull;
+    S.tr_mi = it;
+    S.tr_mp = pu;
   }
 }
 
@@ -1047,6 +1116,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   c.rank = blockIdx.x % P.gsize;
   c.deadline = gtimer() + P.timeout_ns;
   c.edges = 0;
+  c.edges_mark = 0;
   PhGroup *G = grp_of(P, c);
   unsigned long long cy_work = 0, cy_wait = 0, cy_lead = 0, nphase = 0;
   const long long cy0 = clock64();
@@ -1057,6 +1127,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     S.D.q = 0u;
     S.st_items = S.st_stale = S.st_heavy = S.st_repush = S.st_pushes = S.st_chunks = 0;
     S.st_hubs = S.st_solo = 0;
+    S.tr_e = S.tr_mi = S.tr_mp = 0ull;
     for (int i = 0; i < 8; ++i) S.cy[i] = 0ull;
   }
   if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
@@ -1066,9 +1137,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     run_phase<FLT, BLOCK, UU>(P, c, S, false);
     const long long t1 = clock64();
     cy_work += (unsigned long long)(t1 - t0);
+    const bool tracing = P.trace != nullptr && c.gi == 0u;
+    if (tracing) trace_account<BLOCK, UU>(P, c, S);
     /* group barrier: the last CTA in becomes the leader */
     __syncthreads();
     if (tid == 0) {
+      if (tracing) atomicCAS(&G->tr_first, 0ull, gtimer());
       __threadfence();
       const unsigned old = atomicAdd(&G->arrive, 1u);
       S.leader = (old == P.gsize - 1u) ? 1u : 0u;
@@ -1095,6 +1169,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
           }
         }
         run_phase<FLT, BLOCK, UU>(P, c, S, true);
+        if (tracing) trace_account<BLOCK, UU>(P, c, S);
         __syncthreads();
         if (tid == 0) __threadfence();
         __syncthreads();
@@ -1129,6 +1204,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
           S.D.per = ld_rlx32(&dp->per);
           S.D.epoch = ld_rlx32(&dp->epoch);
           S.D.nx = ld_rlx32(&dp->nx);
+          S.D.full = ld_rlx32(&dp->full);
           for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
             S.D.xl[r] = ld_rlx32(&dp->xl[r]);
             S.D.xlo[r] = ld_rlx64(&dp->xlo[r]);
@@ -1385,6 +1461,7 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   if (P->hub_chunk < E.hub_eff) return -9; /* engine sized for longer chunks */
   P->solo_max = k.solo_max;
   P->adapt = k.adapt;
+  P->lh_adapt = k.lh_adapt;
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

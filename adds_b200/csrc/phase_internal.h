@@ -80,7 +80,8 @@ struct __align__(64) PhDesc {
   unsigned nx;
   unsigned xl[PH_MAXR - 1];
   unsigned long long xlo[PH_MAXR - 1], xhi[PH_MAXR - 1];
-  unsigned pad[4];
+  unsigned full;               /* light phase relaxes whole rows, no SETTLED */
+  unsigned pad[3];
 };
 
 /* Per-group state.  `arrive` and `gen` sit in lines of their own; the list
@@ -112,7 +113,13 @@ struct __align__(128) PhGroup {
   unsigned base;               /* absolute base bucket                       */
   unsigned mode;               /* mode of the phase that just ran            */
   unsigned epoch;              /* phases decided so far                      */
-  unsigned pad5[28];
+  /* trace of group 0 only: the running phase's work and its first arrival */
+  unsigned long long tr_first, tr_edges, tr_items, tr_pushes;
+  /* adaptive light/heavy: entries of the bucket's last light phase, light
+   * phases run in it, whether it re-improved many of its own vertices */
+  unsigned long long lh_prev;
+  unsigned lh_k, lh_dense;
+  unsigned pad5[16];
   unsigned long long head[PH_NLIST];
   PhTail tails[PH_NLIST];
 };
@@ -141,6 +148,10 @@ struct PhTrace {
   unsigned count;           /* entries (hub: chunk records; init: vertices)   */
   unsigned short mode;      /* PH_M_* | 0x100 if run by the leader alone      */
   unsigned short base;      /* low 16 bits of the base bucket                 */
+  unsigned edges;           /* edges the phase relaxed                        */
+  unsigned items;           /* entries and records it prepared                */
+  unsigned pushes;          /* entries it appended                           */
+  unsigned tail_ns;         /* first CTA at the barrier to the decision       */
 };
 
 /* Kernel parameters (by value). */
@@ -163,6 +174,7 @@ struct PhParams {
   unsigned hub_chunk;          /* edges per split chunk                       */
   unsigned solo_max;           /* frontiers up to this size run on the leader */
   unsigned adapt;              /* merge thin bucket slots into one phase      */
+  unsigned lh_adapt;           /* whole rows in light phases of sparse buckets */
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
@@ -201,7 +213,7 @@ struct PhKnobs {
   int variant;        /* kernel variant (threads x CTAs per SM), phase.cu      */
   int ctas_per_sm;    /* <= 0: as many as fit                                 */
   int group_ctas;     /* CTAs per group (batches); <= 0: automatic            */
-  unsigned hub_threshold, hub_chunk, solo_max, adapt;
+  unsigned hub_threshold, hub_chunk, solo_max, adapt, lh_adapt;
   unsigned long long timeout_ns;
 };
 

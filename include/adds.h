@@ -75,7 +75,11 @@ typedef struct adds_opts {
                             0 = always go through the HBM queues              */
   int32_t light_heavy;   /* 1: relax heavy edges (w >= delta) once per settled
                             vertex from a weight-sorted row copy; 0: off;
-                            <0 = auto (on)                                     */
+                            2 (phase engine): per bucket — split rows while a
+                            bucket keeps re-improving its own vertices, whole
+                            rows in one light phase once buckets turn sparse
+                            (the asynchronous engine treats 2 as 1);
+                            <0 = auto (2 phase engine, 1 async)              */
   int32_t block_threads; /* threads per persistent CTA: async engine 128, 256 or
                             512; phase engine 256, 512 or 1024; 0 = auto       */
   int32_t greed;         /* async engine: a claim takes avail / (CTAs >> greed)
@@ -285,6 +289,11 @@ typedef struct adds_phase_trace {
   uint16_t mode;  /* 0 init, 1 light, 2 heavy, 3 split rows, 4 exit;
                      | 0x100 when one CTA ran it alone                      */
   uint16_t base;  /* low 16 bits of the bucket being settled                */
+  uint32_t edges;   /* edges the phase relaxed                              */
+  uint32_t items;   /* frontier entries and split-row records it prepared   */
+  uint32_t pushes;  /* entries it appended to the bucket lists               */
+  uint32_t tail_ns; /* from the first CTA reaching the phase's barrier to the
+                       next decision: the phase's load imbalance (0 solo)   */
 } adds_phase_trace;
 /* Records up to cap phases of each later plain solve on g (0 = off). */
 int adds_graph_trace(adds_graph *g, uint32_t cap);

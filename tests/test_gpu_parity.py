@@ -55,7 +55,7 @@ def test_any_delta_gives_same_distances(engine, shift, lh):
 
 @pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("solo", [0, 64, 100000])
-@pytest.mark.parametrize("lh", [0, 1])
+@pytest.mark.parametrize("lh", [0, 1, 2])
 def test_phase_schedules_int_rmat(variant, solo, lh):
     """Kernel variants, solo-CTA thresholds (0: never, 100000: whole solve on
     one CTA) and split rows (hub threshold 64 edges) all give the oracle's
@@ -98,12 +98,16 @@ def test_phase_trace_and_stats():
     modes = tr["mode"] & 0xFF
     assert modes[0] == 0 and modes[-1] == 4  # init first, exit last
     assert ((tr["mode"] & 0x100) != 0).sum() == st["solo_phases"]
+    # per-phase work adds up to the solve's counters
+    assert int(tr["edges"].astype(np.int64).sum()) == st["edges_scanned"]
+    assert int(tr["pushes"].astype(np.int64).sum()) <= st["pushes"]
+    assert (tr["tail_ns"][(tr["mode"] & 0x100) != 0] == 0).all()
     assert st["items_popped"] >= st["items_stale"] and st["edges_scanned"] > 0
     assert st["engine"] == PHASE and st["ctas"] > 0
 
 
 @pytest.mark.parametrize("variant", VARIANTS[:3])
-@pytest.mark.parametrize("lh", [0, 1])
+@pytest.mark.parametrize("lh", [0, 1, 2])
 def test_phase_schedules_float_grid(variant, lh):
     g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=8)
     for shift in (6, 12, 16, 20):
@@ -113,7 +117,7 @@ def test_phase_schedules_float_grid(variant, lh):
 
 @pytest.mark.parametrize("adapt", [0, 1])
 @pytest.mark.parametrize("solo", [0, 64])
-@pytest.mark.parametrize("lh", [0, 1])
+@pytest.mark.parametrize("lh", [0, 1, 2])
 def test_phase_bucket_widening(adapt, solo, lh):
     """The leader widens a bucket over up to four thin consecutive slots
     (adapt 1): the distances stay the oracle's, int32 and float32, with the
@@ -153,6 +157,18 @@ def test_phase_bucket_widening_merges_thin_slots():
     light = (tr["mode"] & 0xFF) == 1
     steps = np.diff(tr["base"].astype(np.int64))[light[1:]]
     assert (steps > 1).any()
+
+
+def test_adaptive_light_heavy_saves_phases():
+    """light_heavy 2 relaxes whole rows once buckets turn sparse: the same
+    distances as the split schedule in fewer phases, with no more than a few
+    percent more edges (vertices re-improved inside a sparse bucket relax
+    their heavy edges twice)."""
+    g = G.rmat(17, 16, seed=31, w_hi=10000)
+    src = G.max_degree_vertex(g)
+    st = {lh: _check(g, src, engine=PHASE, delta_shift=10, light_heavy=lh) for lh in (1, 2)}
+    assert st[2]["phases"] < st[1]["phases"]
+    assert st[2]["edges_scanned"] <= 1.05 * st[1]["edges_scanned"]
 
 
 def test_phase_float_grid_large_keys():
