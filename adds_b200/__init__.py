@@ -131,6 +131,19 @@ class Graph:
                               C.byref(st)), "adds_sssp")
         return out, st.as_dict()
 
+    def sssp_sources(self, srcs, outs, opts: Opts | None = None) -> dict:
+        """One solve per source, result i copied into outs[i] (host or device
+        buffers of n words; an address repeats to reuse a buffer) while solve
+        i+1 runs; returns the stats."""
+        st = Stats()
+        ss = (C.c_uint32 * len(srcs))(*[int(s) for s in srcs])
+        ps = (C.c_void_p * len(outs))(*[_ptr(o) for o in outs])
+        if len(outs) != len(srcs):
+            raise ValueError("one output buffer per source")
+        check(lib().adds_sssp_sources(self._h, ss, len(srcs), ps, C.byref(opts) if opts else None,
+                                      C.byref(st)), "adds_sssp_sources")
+        return st.as_dict()
+
     def sssp_async(self, src: int, opts: Opts | None = None) -> None:
         check(lib().adds_sssp_async(self._h, src, C.byref(opts) if opts else None),
               "adds_sssp_async")

@@ -146,6 +146,8 @@ SIGNATURES = [
     ("adds_graph_generate", C.c_int, [C.POINTER(GenSpec), C.c_int, C.POINTER(C.c_void_p)]),
     ("adds_sssp", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(Opts), C.POINTER(Stats)]),
     ("adds_sssp_async", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Opts)]),
+    ("adds_sssp_sources", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32,
+                                     C.POINTER(C.c_void_p), C.POINTER(Opts), C.POINTER(Stats)]),
     ("adds_graph_sync", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("adds_graph_last_dist", C.c_int, [C.c_void_p, C.c_void_p]),
     ("adds_graph_reached", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

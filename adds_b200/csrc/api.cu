@@ -411,6 +411,14 @@ struct adds_graph {
   Knobs last_knobs;
   EngParams last_params;
   int pending = 0; /* async solves enqueued since the last sync */
+  /* their sources and options: adds_graph_sync runs them again, on a grown
+   * worklist pool, when one of them ran out of worklist space */
+  std::vector<std::pair<uint32_t, adds_opts>> pend;
+  /* adds_sssp_sources: two staging copies of dist, the copy-out stream and
+   * its events (made on first use) */
+  unsigned *stage = nullptr;
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
   /* per-solve event ring: (start, kernel start, kernel end, end) */
   static constexpr int kRing = 256;
   cudaEvent_t ring[kRing][4] = {};
@@ -545,6 +553,13 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->sort_tmp) cudaFree(g->sort_tmp);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->cstream) cudaStreamSynchronize(g->cstream);
+  if (g->stage) cudaFree(g->stage);
+  for (int j = 0; j < 2; ++j) {
+    if (g->ev_free[j]) cudaEventDestroy(g->ev_free[j]);
+    if (g->ev_ready[j]) cudaEventDestroy(g->ev_ready[j]);
+  }
+  if (g->cstream) cudaStreamDestroy(g->cstream);
   for (int i = 0; i < adds_graph::kRing; ++i)
     for (int j = 0; j < 4; ++j)
       if (g->ring[i][j]) cudaEventDestroy(g->ring[i][j]);
@@ -1142,6 +1157,7 @@ extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds
   int retries = 0;
   CK(cudaStreamSynchronize(st));
   g->ring_used = 0;
+  g->pend.clear();
   for (;;) {
     rc = sssp_enqueue(g, src, opts);
     if (rc) return rc;
@@ -1184,6 +1200,110 @@ extern "C" int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds
   return ADDS_OK;
 }
 
+/* Solves srcs[0..ns) one after another and copies result i to dist_out[i]
+ * while solve i+1 runs: the result is copied on the device into one of two
+ * staging buffers, and a second stream moves it to host memory, so the
+ * device-to-host transfer overlaps the next solve instead of following it.
+ * The host loop enqueues solve i before it hands result i-1 to the copy
+ * stream, so a pageable destination (whose copy blocks the host) overlaps
+ * as well.  A device destination is copied on the solve stream. */
+extern "C" int adds_sssp_sources(adds_graph *g, const uint32_t *srcs, uint32_t ns,
+                                 void *const *dist_out, const adds_opts *opts,
+                                 adds_stats *stats) {
+  if (!g || (ns && (!srcs || !dist_out))) return ADDS_ERR_INVALID;
+  for (uint32_t i = 0; i < ns; ++i)
+    if (srcs[i] >= g->n || !dist_out[i]) return ADDS_ERR_INVALID;
+  int rc = set_device(g->device);
+  if (rc) return rc;
+  if (ns == 0) return ADDS_OK;
+  const size_t bytes = (size_t)g->n * 4;
+  cudaStream_t st = pick_stream(g, opts);
+  CK(cudaStreamSynchronize(st));
+  g->ring_used = 0;
+  g->pend.clear();
+  if (!g->stage) CK(cudaMalloc(&g->stage, 2 * (bytes ? bytes : 4)));
+  if (!g->cstream) CK(cudaStreamCreateWithFlags(&g->cstream, cudaStreamNonBlocking));
+  for (int j = 0; j < 2; ++j) {
+    if (!g->ev_free[j]) CK(cudaEventCreateWithFlags(&g->ev_free[j], cudaEventDisableTiming));
+    if (!g->ev_ready[j]) CK(cudaEventCreateWithFlags(&g->ev_ready[j], cudaEventDisableTiming));
+  }
+  bool staged[2] = {false, false};
+  /* result i, staged in buffer i & 1, to the caller on the copy stream */
+  auto copy_out = [&](uint32_t i) -> int {
+    const int j = (int)(i & 1u);
+    CK(cudaStreamWaitEvent(g->cstream, g->ev_ready[j], 0));
+    CK(cudaMemcpyAsync(dist_out[i], g->stage + (size_t)j * g->n, bytes,
+                       cudaMemcpyDeviceToHost, g->cstream));
+    CK(cudaEventRecord(g->ev_free[j], g->cstream));
+    return ADDS_OK;
+  };
+  int pending_out = -1; /* the staged result not yet handed to the copy stream */
+  for (uint32_t i = 0; i < ns && !rc; ++i) {
+    rc = sssp_enqueue(g, srcs[i], opts);
+    if (rc) break;
+    /* solve i is queued: now the previous result may leave */
+    if (pending_out >= 0) {
+      rc = copy_out((uint32_t)pending_out);
+      pending_out = -1;
+      if (rc) break;
+    }
+    if (is_device_ptr(dist_out[i])) {
+      CK(cudaMemcpyAsync(dist_out[i], g->dist, bytes, cudaMemcpyDeviceToDevice, st));
+      continue;
+    }
+    const int j = (int)(i & 1u);
+    if (staged[j]) CK(cudaStreamWaitEvent(st, g->ev_free[j], 0));
+    CK(cudaMemcpyAsync(g->stage + (size_t)j * g->n, g->dist, bytes, cudaMemcpyDeviceToDevice,
+                       st));
+    CK(cudaEventRecord(g->ev_ready[j], st));
+    staged[j] = true;
+    pending_out = (int)i;
+  }
+  if (!rc && pending_out >= 0) rc = copy_out((uint32_t)pending_out);
+  const cudaError_t e1 = cudaStreamSynchronize(st);
+  const cudaError_t e2 = cudaStreamSynchronize(g->cstream);
+  if (rc) {
+    g->ring_used = 0;
+    return rc;
+  }
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return cuda_fail(e1 != cudaSuccess ? e1 : e2, "multi-source solve");
+  const bool phase = g->last_engine == ADDS_ENGINE_PHASE;
+  rc = phase ? phase_status(g->peng) : engine_status(g->eng);
+  if (rc == ADDS_ERR_WL_OVERFLOW) {
+    /* the worklist outgrew its pool: solve one at a time, which regrows it */
+    g->ring_used = 0;
+    if (phase) ph_engine_reset(g->peng, st); else engine_full_reset(g->eng, st);
+    for (uint32_t i = 0; i < ns; ++i) {
+      rc = adds_sssp(g, srcs[i], dist_out[i], opts, i + 1 == ns ? stats : nullptr);
+      if (rc) return rc;
+    }
+    return ADDS_OK;
+  }
+  if (rc) {
+    if (phase) ph_engine_reset(g->peng, st); else engine_full_reset(g->eng, st);
+    g->ring_used = 0;
+    return rc;
+  }
+  double ms = 0, kms = 0;
+  ring_times(g, &ms, &kms);
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->ms = ms;
+    stats->kernel_ms = kms;
+    if (phase) {
+      fill_phase_stats(g->peng, stats);
+      stats->delta_shift = (int32_t)g->peng.qs_host[0].shift;
+    } else {
+      fill_stats(g->eng, g->last_params, stats);
+      stats->delta_shift = (int32_t)g->eng.qs_host[0].shift0;
+      stats->engine = ADDS_ENGINE_ASYNC;
+    }
+  }
+  g->pending = 0;
+  return ADDS_OK;
+}
+
 /* Asynchronous form for back-to-back solves: errors surface in
  * adds_graph_sync (a failed solve makes the following ones exit at once). */
 extern "C" int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opts) {
@@ -1191,7 +1311,12 @@ extern "C" int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opt
   int rc = set_device(g->device);
   if (rc) return rc;
   rc = sssp_enqueue(g, src, opts);
-  if (!rc) ++g->pending;
+  if (!rc) {
+    ++g->pending;
+    adds_opts o;
+    if (opts) o = *opts; else adds_opts_init(&o);
+    g->pend.emplace_back(src, o);
+  }
   return rc;
 }
 
@@ -1206,6 +1331,21 @@ extern "C" int adds_graph_sync(adds_graph *g, adds_stats *stats) {
   if (phase ? g->peng.nq == 0 : g->eng.nq == 0) return ADDS_OK;
   rc = phase ? phase_status(g->peng) : engine_status(g->eng);
   g->pending = 0;
+  std::vector<std::pair<uint32_t, adds_opts>> redo;
+  redo.swap(g->pend);
+  if (rc == ADDS_ERR_WL_OVERFLOW && !redo.empty()) {
+    /* a solve outgrew the worklist pool (and the ones after it exited):
+     * run them all again one at a time, as adds_sssp does, on a larger pool;
+     * the graph then holds the last one's distances as it would have */
+    if (phase) ph_engine_free(g->peng); else engine_free(g->eng);
+    g->grow *= 2;
+    for (size_t i = 0; i < redo.size(); ++i) {
+      rc = adds_sssp(g, redo[i].first, nullptr, &redo[i].second,
+                     i + 1 == redo.size() ? stats : nullptr);
+      if (rc) return rc;
+    }
+    return ADDS_OK;
+  }
   if (rc) {
     if (phase) ph_engine_reset(g->peng, g->stream); else engine_full_reset(g->eng, g->stream);
     return rc;

@@ -287,19 +287,21 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
     if prof and "dram_bytes_per_launch" in prof:
         traffic = prof["dram_bytes_per_launch"]
     # e2e: the C-ABI call with a pinned host output buffer, copies timed
-    pinned = torch.empty(g.n, dtype=torch.int32, pin_memory=True)
     e2e_steps = steps[: max(1, min(len(steps), args.e2e_steps))]
+    pinned = [torch.empty(g.n, dtype=torch.int32, pin_memory=True) for _ in e2e_steps]
+    g.sssp_sources(e2e_steps[:2], pinned[:2], opts)  # staging buffers made outside the timing
     barrier(dist, local)
     te0 = time.perf_counter()
-    for s in e2e_steps:
-        g.sssp(s, opts, out=pinned.data_ptr())
+    g.sssp_sources(e2e_steps, pinned, opts)
     te1 = time.perf_counter()
     e2e_units = sum(mr[s] for s in e2e_steps)
     etmax, eusum = reduce_max_sum(dist, local, te1 - te0, e2e_units)
     e2e = {"value": eusum / etmax / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 4,
            "d2h_bytes_per_step": 4 * g.n,
-           "note": "adds_sssp(graph, src, pinned host dist) per step, host wall clock; the "
-                   "4-byte source id is the step input, the distance array the result"}
+           "note": "adds_sssp_sources(graph, sources, one pinned host distance array per "
+                   "step): each step's result is copied to host memory while the next step "
+                   "solves; host wall clock; the 4-byte source id is the step input, the "
+                   "distance array the result"}
     work_edges = st["edges_scanned"]
     if args.trace:  # one more solve with the phase trace on (outside the timed region)
         g.trace(1 << 16)

@@ -203,12 +203,24 @@ int adds_sssp(adds_graph *g, uint32_t src, void *dist_out, const adds_opts *opts
               adds_stats *stats);
 /* Enqueues a solve on the graph's stream and returns at once (no host
  * synchronisation); adds_graph_sync waits for all enqueued solves and
- * reports the first device error.  The distances of the last solve stay in
- * the graph. */
+ * reports the first device error.  A solve that ran out of worklist space
+ * (ADDS_ERR_WL_OVERFLOW) is not an error there: the pool grows and the
+ * enqueued solves run again one at a time, as adds_sssp does.  The
+ * distances of the last solve stay in the graph. */
 int adds_sssp_async(adds_graph *g, uint32_t src, const adds_opts *opts);
 int adds_graph_sync(adds_graph *g, adds_stats *stats);
 /* Copies the distances of the last solve on g (host or device pointer). */
 int adds_graph_last_dist(adds_graph *g, void *dist_out);
+/* Several sources on one graph, one solve each, result i in dist_out[i]
+ * (n words each, host or device; an entry may repeat a buffer, later results
+ * overwrite earlier ones).  Replaces the reference's one-process-per-source
+ * loop (run_all.sh:4-18 calls `sssp -s <src>` per source; gg_main,
+ * ads_int/kernel.cu:185-288, copies the result back after the solve): here
+ * the copy of result i to host memory runs on a second stream while solve
+ * i+1 runs.  stats sums the solve times; the other counters are the last
+ * solve's. */
+int adds_sssp_sources(adds_graph *g, const uint32_t *srcs, uint32_t ns, void *const *dist_out,
+                      const adds_opts *opts, adds_stats *stats);
 /* Fills stats->reached and stats->reached_edges for the last solve on g. */
 int adds_graph_reached(adds_graph *g, uint64_t *reached, uint64_t *reached_edges);
 

@@ -46,6 +46,38 @@ def test_erdos_renyi_int(engine):
 
 
 @pytest.mark.parametrize("engine", [ASYNC, PHASE])
+def test_sources_overlapped_copy_out(engine):
+    """adds_sssp_sources: results of several sources into pageable, pinned
+    and device buffers, one buffer reused (the later result wins), each equal
+    to the oracle's distances for its source."""
+    import torch
+    g = G.rmat(14, 16, seed=5, w_hi=5000)
+    deg = np.diff(g.row.astype(np.int64))
+    srcs = [int(x) for x in np.random.default_rng(3).choice(np.flatnonzero(deg > 0), 6,
+                                                             replace=False)]
+    dg = A.Graph.from_csr(g)
+    try:
+        pageable = [np.full(g.n, 7, dtype=np.uint32) for _ in range(2)]
+        pinned = torch.full((g.n,), 7, dtype=torch.int32).pin_memory()
+        dev = torch.full((g.n,), 7, dtype=torch.int32, device="cuda")
+        reuse = np.full(g.n, 7, dtype=np.uint32)
+        outs = [pageable[0], pinned, dev, reuse, pageable[1], reuse]
+        st = dg.sssp_sources(srcs, outs, A.default_opts(engine=engine, **OPTS))
+        assert st["engine"] == engine and st["kernel_ms"] > 0
+        got = [pageable[0], pinned.numpy().view(np.uint32), dev.cpu().numpy().view(np.uint32),
+               None, pageable[1], reuse]
+        for s, d in zip(srcs, got):
+            if d is None:
+                continue
+            ref, _ = O.dijkstra(g, s)
+            assert np.array_equal(d, ref), s
+        # the last solve's distances also stay in the graph
+        assert np.array_equal(dg.last_dist(), reuse)
+    finally:
+        dg.close()
+
+
+@pytest.mark.parametrize("engine", [ASYNC, PHASE])
 @pytest.mark.parametrize("shift", [0, 4, 9, 14, 20])
 @pytest.mark.parametrize("lh", [0, 1])
 def test_any_delta_gives_same_distances(engine, shift, lh):
