@@ -322,6 +322,8 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
                      "kernel": ("adds_phase::phase_kernel" if st["engine"] == 2 else
                                 "adds::solve_kernel") + " (persistent, 1 launch per solve)",
                      "traffic_note": (prof or {}).get("scaled_by"),
+                     "dram_gbs": (traffic / (kernel_s / args.steps) / 1e9) if traffic else None,
+                     "l2_hit_rate_pct": (prof or {}).get("l2_hit_rate_pct"),
                      "bytes_model": "12*m_r + 24*n_r per solve"},
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
