@@ -1221,7 +1221,10 @@ extern "C" int adds_sssp_sources(adds_graph *g, const uint32_t *srcs, uint32_t n
   CK(cudaStreamSynchronize(st));
   g->ring_used = 0;
   g->pend.clear();
-  if (!g->stage) CK(cudaMalloc(&g->stage, 2 * (bytes ? bytes : 4)));
+  if (!g->stage) {
+    CK(cudaMalloc(&g->stage, 2 * (bytes ? bytes : 4)));
+    g->bytes += 2 * bytes;
+  }
   if (!g->cstream) CK(cudaStreamCreateWithFlags(&g->cstream, cudaStreamNonBlocking));
   for (int j = 0; j < 2; ++j) {
     if (!g->ev_free[j]) CK(cudaEventCreateWithFlags(&g->ev_free[j], cudaEventDisableTiming));
