@@ -157,6 +157,7 @@ struct PSmem {
                                waits), expand, flush, barrier wait, leader,
                                grid-phase work, total */
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
+  unsigned hub_made; /* this CTA cut a row into records in the current phase */
   unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
 };
 
@@ -395,6 +396,7 @@ __device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOC
     const unsigned deg = re - rb;
     const unsigned nch = (deg + P.hub_chunk - 1u) / P.hub_chunk;
     const unsigned hb = atomicAdd(&G->hub_count, nch);
+    S.hub_made = 1u;
     if (hb + nch > P.hub_cap) {
       raise_err(P.g, PH_ERR_HUB_OVERFLOW, W_HUB);
     } else {
@@ -776,6 +778,7 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
   /* frontier chunks first, then split-row records (a records-only phase
    * finishes what a solo phase left) */
   bool records = mode == PH_M_HUB;
+  if (tid == 0) S.hub_made = 0u; /* read after the claim barriers below */
   long long t0 = clock64();
   for (;;) {
     const bool have = records ? prepare_records<FLT, BLOCK, UU>(P, c, S)
@@ -791,6 +794,8 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
       /* no frontier chunk left for this CTA: it appends no more split rows,
        * and helps expand the ones the group has appended */
       records = true;
+      /* alone and without records: nothing is left for this phase */
+      if (solo && S.hub_made == 0u) break;
       if (tid == 0) {
         __threadfence();
         PhGroup *G = grp_of(P, c);
@@ -1153,7 +1158,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
         if (!solo_ok<BLOCK, UU>(P, S)) break;
         if (tid == 0) {
           st_rlx32(&G->producers, 1u); /* this CTA alone expands the phase */
-          __threadfence();
           __threadfence();
           ++S.st_solo;
           if (P.trace && c.gi == 0u) { /* mark the record just written as solo */
