@@ -81,6 +81,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def clock_dir():
+    """Where the nvidia-smi clock samples of the timed region are written
+    (ADDS_BENCH_OUT, else the temporary directory)."""
+    import tempfile
+    return os.environ.get("ADDS_BENCH_OUT") or tempfile.gettempdir()
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -254,8 +261,7 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
     torch.cuda.set_device(local)
     barrier(dist, local)
     torch.cuda.synchronize(local)
-    smi = ClockSampler(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else "/tmp", f"clocks_rank{rank}.csv"))
+    smi = ClockSampler(local, os.path.join(clock_dir(), f"clocks_rank{rank}.csv"))
     t0 = time.perf_counter()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -433,8 +439,7 @@ def run_batched(args, ws, rank, local, dist):
     torch.cuda.set_device(local)
     barrier(dist, local)
     torch.cuda.synchronize(local)
-    smi = ClockSampler(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else "/tmp", f"clocks_batched_rank{rank}.csv"))
+    smi = ClockSampler(local, os.path.join(clock_dir(), f"clocks_batched_rank{rank}.csv"))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     torch.cuda.synchronize(local)
