@@ -58,7 +58,8 @@ class Opts(C.Structure):
         ("engine", C.c_int32),
         ("group_ctas", C.c_int32),
         ("solo_max", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("near_far", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -266,7 +266,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
-  int engine, variant, group_ctas, solo_max; /* phase engine */
+  int engine, variant, group_ctas, solo_max, near_far; /* phase engine */
   unsigned long long timeout_ns;
 };
 
@@ -289,6 +289,7 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.solo_max = (unsigned)std::max(0, k.solo_max);
   p.adapt = k.adapt > 0 ? 1u : 0u;
   p.lh_adapt = k.light_heavy == 2 ? 1u : 0u;
+  p.near_far = k.near_far ? 1u : 0u;
   p.timeout_ns = k.timeout_ns;
   return p;
 }
@@ -848,6 +849,7 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
 
   k->strict = o->strict_order >= 0 ? o->strict_order : (t->strict_order >= 0 ? t->strict_order : 1);
   k->local_max = o->local_max >= 0 ? o->local_max : (t->local_max >= 0 ? t->local_max : 512);
+  k->near_far = (o->near_far > 0 || t->near_far > 0) ? 1 : 0;
   k->block = o->block_threads > 0 ? o->block_threads : (t->block_threads > 0 ? t->block_threads : 256);
   k->greed = o->greed >= 0 ? o->greed : (t->greed >= 0 ? t->greed : 4);
   k->engine = o->engine > 0 ? o->engine : (t->engine > 0 ? t->engine : ADDS_ENGINE_PHASE);

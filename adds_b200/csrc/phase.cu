@@ -108,9 +108,11 @@ __device__ __forceinline__ unsigned bucket_of(unsigned d, float scale, unsigned 
   if (FLT) key = __float2uint_rz(__fmul_rn(__uint_as_float(d), scale));
   return key >> shift;
 }
-/* list of a push with bucket b relative to the base bucket being settled */
-__device__ __forceinline__ unsigned route(unsigned b, unsigned base) {
+/* list of a push with bucket b relative to the base bucket being settled;
+ * the near-far schedule keeps one far pile instead of the ring */
+__device__ __forceinline__ unsigned route(unsigned b, unsigned base, unsigned near_far) {
   if (b <= base) return PH_LNEXT;
+  if (near_far) return PH_LFAR;
   const unsigned off = min(b - base, (unsigned)PH_NSLOT - 1u);
   return (base + off) & (PH_NSLOT - 1u);
 }
@@ -377,7 +379,14 @@ __device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOC
   }
   const unsigned b = bucket_of<FLT>(d, Q.scale, Q.shift);
   if (b > d_base) { /* left in the far slot: move it to its own bucket */
-    stage<BLOCK, UU>(S, v, d, route(b, d_base));
+    stage<BLOCK, UU>(S, v, d, route(b, d_base, P.near_far));
+    if (P.near_far) {
+      /* near-far: the smallest bucket the split sends back to the pile is
+       * where the leader may move the threshold next */
+      const unsigned am = __activemask();
+      const unsigned wm = __reduce_min_sync(am, b);
+      if ((threadIdx.x & 31u) == (unsigned)(__ffs(am) - 1)) atomicMin(&G->far_min, wm);
+    }
     ++nrepush;
     return;
   }
@@ -734,7 +743,8 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
     for (int u = 0; u < U; ++u) {
       if (nd[u] < cur[u]) {
         red_min(dist + dst[u], nd[u]);
-        stage<BLOCK, UU>(S, dst[u], nd[u], route(bucket_of<FLT>(nd[u], scale, shift), base));
+        stage<BLOCK, UU>(S, dst[u], nd[u],
+                         route(bucket_of<FLT>(nd[u], scale, shift), base, P.near_far));
       }
     }
     if ((it % PSmem<BLOCK, UU>::SEGI) == PSmem<BLOCK, UU>::SEGI - 1u || it + 1u == nit) {
@@ -857,6 +867,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       if (list_reserve(P, c, PH_LNEXT, 1u, &b, pg, &cvp, &cpi))
         st_rlx64(entry_ptr(P, c, pg[0], b), (unsigned long long)src);
       st_rlx32(&G->base, 0u);
+      st_rlx32(&G->far_min, 0xFFFFFFFFu);
       /* the source's bucket counts as dense: it starts with split rows */
       st_rlx32(&G->lh_dense, 1u);
       st_rlx32(&G->lh_k, 0u);
@@ -907,6 +918,34 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       list = PH_LSETTLED;
       lo = hs;
       hi = ts;
+    } else if (P.near_far) {
+      /* near-far: the threshold moves up one bucket, or to the smallest
+       * bucket pushed to the far pile since it last moved, and the pile is
+       * split against it (entries above it are pushed to the pile again) */
+      const unsigned long long tf = ld_rlx64(&G->tails[PH_LFAR].tail);
+      const unsigned long long hf = ld_rlx64(&G->head[PH_LFAR]);
+      if (tf > hf) {
+        const unsigned fm = ld_rlx32(&G->far_min);
+        mode = PH_M_LIGHT;
+        list = PH_LFAR;
+        lo = hf;
+        hi = tf;
+        base = (fm != 0xFFFFFFFFu && fm > base + 1u) ? fm : base + 1u;
+        if (lane == 0) {
+          st_rlx32(&G->base, base);
+          st_rlx32(&G->far_min, 0xFFFFFFFFu);
+        }
+        if (P.lh_adapt) {
+          full = ld_rlx32(&G->lh_dense) != 0u ? 0u : 1u;
+          if (lane == 0) {
+            st_rlx32(&G->lh_dense, 0u);
+            st_rlx64(&G->lh_prev, tf - hf);
+            st_rlx32(&G->lh_k, 1u);
+          }
+        }
+      } else {
+        next_query = true;
+      }
     } else {
       /* advance: the nearest non-empty slot above the base */
       const unsigned offa = lane + 1u, offb = lane + 33u;
@@ -1459,6 +1498,7 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->solo_max = k.solo_max;
   P->adapt = k.adapt;
   P->lh_adapt = k.lh_adapt;
+  P->near_far = k.near_far ? 1u : 0u;
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

@@ -28,6 +28,7 @@
 #define PH_LNEXT PH_NSLOT          /* list: current bucket's next frontier     */
 #define PH_LSETTLED (PH_NSLOT + 1) /* list: settled vertices with heavy edges  */
 #define PH_NLIST (PH_NSLOT + 2)
+#define PH_LFAR (PH_NSLOT - 1)     /* near-far schedule: the far pile          */
 #define PH_PAGE_LOG2 12
 #define PH_PAGE (1u << PH_PAGE_LOG2) /* entries per pool page (8 B each)      */
 
@@ -119,7 +120,10 @@ struct __align__(128) PhGroup {
    * phases run in it, whether it re-improved many of its own vertices */
   unsigned long long lh_prev;
   unsigned lh_k, lh_dense;
-  unsigned pad5[16];
+  /* near-far schedule: smallest bucket pushed to the far list since the
+   * threshold last moved */
+  unsigned far_min;
+  unsigned pad5[15];
   unsigned long long head[PH_NLIST];
   PhTail tails[PH_NLIST];
 };
@@ -175,6 +179,7 @@ struct PhParams {
   unsigned solo_max;           /* frontiers up to this size run on the leader */
   unsigned adapt;              /* merge thin bucket slots into one phase      */
   unsigned lh_adapt;           /* whole rows in light phases of sparse buckets */
+  unsigned near_far;           /* two lists instead of the bucket ring         */
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
@@ -214,6 +219,7 @@ struct PhKnobs {
   int ctas_per_sm;    /* <= 0: as many as fit                                 */
   int group_ctas;     /* CTAs per group (batches); <= 0: automatic            */
   unsigned hub_threshold, hub_chunk, solo_max, adapt, lh_adapt;
+  unsigned near_far;  /* near-far schedule instead of the bucket ring          */
   unsigned long long timeout_ns;
 };
 

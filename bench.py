@@ -614,6 +614,52 @@ def run_ceiling(args, ws, rank, local):
                        for k, v in zip(names, ms)}}
 
 
+def run_comparators(args, ws, rank, local):
+    """The schedules of the reference's comparison set run in this engine on
+    one R-MAT 22 graph (the Galois GPU nf and nvGraph nv binaries cannot be
+    built here): delta-stepping, the reference's asynchronous bucket
+    schedule, near-far (nf_int.patch: one far pile split against a moving
+    threshold) and frontier Bellman-Ford (nv_int/kernel.cu's schedule), all
+    at the same bucket width.  One synchronous solve per source after a
+    warm-up; every schedule's distances must equal delta-stepping's."""
+    import adds_b200 as A
+    wl = WORKLOADS["rmat22"]
+    g = make_graph(wl, local)
+    row = np.empty(g.n + 1, dtype=np.uint64)
+    A.check(A.lib().adds_graph_download(g.handle, row.ctypes.data, None, None))
+    srcs = pick_sources(g, wl, row)
+    shift = 10
+    scheds = {
+        "delta_stepping": A.default_opts(engine=2, delta_shift=shift),
+        "async_buckets": A.default_opts(engine=1, delta_shift=shift),
+        "near_far": A.default_opts(engine=2, near_far=1, delta_shift=shift, light_heavy=0),
+        "bellman_ford": A.default_opts(engine=2, delta_shift=31, light_heavy=0),
+    }
+    ref, mr = {}, {}
+    for s in srcs:
+        d, _ = g.sssp(s, scheds["delta_stepping"])
+        ref[s] = d
+        mr[s] = g.reached()[1]
+    res = {}
+    for name, o in scheds.items():
+        o.timeout_ms = 20000
+        g.sssp(srcs[0], o)  # warm-up (engine set-up)
+        kms, phases, same = 0.0, 0, True
+        for s in srcs:
+            d, st = g.sssp(s, o)
+            kms += st["kernel_ms"]
+            phases += st["phases"]
+            same = same and bool(np.array_equal(d, ref[s]))
+        res[name] = {"ms_per_solve": kms / len(srcs),
+                     "gteps": sum(mr.values()) / (kms / 1e3) / 1e9,
+                     "phases_per_solve": phases / len(srcs), "same_distances": same}
+    g.close()
+    return {"metric": "sssp_gteps", "unit": "GTEPS", "higher_is_better": True, "n_gpus": ws,
+            "config": {"workload": "comparators: R-MAT 22 int32 U[1,10000], 8 sources, "
+                                   "four schedules in one engine", "delta_shift": shift},
+            "value": res["delta_stepping"]["gteps"], "schedules": res}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -621,7 +667,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat24",
-                    choices=sorted(WORKLOADS) + ["batched", "diff", "ceiling"])
+                    choices=sorted(WORKLOADS) + ["batched", "diff", "ceiling", "comparators"])
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-tune", action="store_true")
@@ -633,9 +679,10 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_env()
-    if args.workload == "ceiling":
+    if args.workload in ("ceiling", "comparators"):
         if rank == 0:
-            print(json.dumps(run_ceiling(args, ws, rank, local)), flush=True)
+            fn = run_ceiling if args.workload == "ceiling" else run_comparators
+            print(json.dumps(fn(args, ws, rank, local)), flush=True)
         return
     if args.workload in ("batched", "diff"):
         if args.impl == "reference":

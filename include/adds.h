@@ -89,7 +89,12 @@ typedef struct adds_opts {
                             together; 0 = auto                                 */
   int32_t solo_max;      /* phase engine: frontiers of at most this many entries
                             run on one CTA without a group barrier; <0 = auto  */
-  int32_t reserved[5];
+  int32_t near_far;      /* phase engine, 1: near-far schedule (the Galois GPU
+                            nf comparator, nf_int.patch): one far pile instead
+                            of the bucket ring, split against a threshold that
+                            moves one bucket at a time (or to the smallest
+                            bucket in the pile); 0 = bucket ring             */
+  int32_t reserved[4];
 } adds_opts;
 
 /* Engines.  PHASE settles the buckets in bulk-synchronous phases (light

@@ -98,6 +98,39 @@ def test_phase_schedules_int_rmat(variant, solo, lh):
                block_threads=variant[0], ctas_per_sm=variant[1], hub_threshold=64)
 
 
+@pytest.mark.parametrize("lh", [0, 1, 2])
+@pytest.mark.parametrize("solo", [0, 64])
+@pytest.mark.parametrize("shift", [6, 10])
+def test_near_far_schedule_int_rmat(lh, solo, shift):
+    """The near-far comparator schedule (one far pile split against a moving
+    threshold) reaches the oracle's distances, re-pushing what stays far."""
+    g = G.rmat(14, 16, seed=9, w_hi=5000)
+    st = _check(g, G.max_degree_vertex(g), engine=PHASE, near_far=1, light_heavy=lh,
+                solo_max=solo, delta_shift=shift)
+    assert st["engine"] == PHASE and st["repushes"] > 0
+
+
+@pytest.mark.parametrize("lh", [0, 2])
+def test_near_far_schedule_float_grid(lh):
+    g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=12)
+    _check(g, 40 * 96 + 48, engine=PHASE, near_far=1, light_heavy=lh)
+
+
+def test_near_far_batch():
+    gs = [G.erdos_renyi(3000 + 500 * i, 8, seed=40 + i) for i in range(5)]
+    dgs = [A.Graph.from_csr(g) for g in gs]
+    try:
+        b = A.Batch(dgs, [1, 2, 3, 4, 5], A.default_opts(engine=PHASE, near_far=1, **OPTS))
+        b.run()
+        for q, g in enumerate(gs):
+            ref, _ = O.dijkstra(g, q + 1)
+            assert np.array_equal(b.dist(q), ref), q
+        b.close()
+    finally:
+        for d in dgs:
+            d.close()
+
+
 @pytest.mark.parametrize("engine", [ASYNC, PHASE])
 @pytest.mark.parametrize("wt", [G.I32, G.F32])
 def test_frontier_bellman_ford(engine, wt):
