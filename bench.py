@@ -332,7 +332,9 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
                      "l2_hit_rate_pct": (prof or {}).get("l2_hit_rate_pct"),
                      "bytes_model": "12*m_r + 24*n_r per solve"},
         "e2e": e2e,
-        "gpu_launches": 2 * args.steps,
+        # phase engine: one persistent kernel per solve; asynchronous engine:
+        # its init kernel and its persistent kernel
+        "gpu_launches": (1 if st["engine"] == 2 else 2) * args.steps,
         "clocks": clocks,
         "extra": {
             "n": g.n, "m": g.m, "sources": srcs, "m_r": [mr[s] for s in srcs],
@@ -488,7 +490,7 @@ def run_batched(args, ws, rank, local, dist):
         "speedup_vs_loop": value / loop_solves_per_s,
         "e2e": {"value": len(qs) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 4 * len(qs),
                 "d2h_bytes_per_step": 4 * tot_n},
-        "gpu_launches": 2 * args.steps, "clocks": clocks,
+        "gpu_launches": (1 if st["engine"] == 2 else 2) * args.steps, "clocks": clocks,
         "extra": {"kernel_ms_per_launch": kms / args.steps},
     }
     b.close()
