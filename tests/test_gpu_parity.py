@@ -98,6 +98,30 @@ def test_phase_schedules_int_rmat(variant, solo, lh):
                block_threads=variant[0], ctas_per_sm=variant[1], hub_threshold=64)
 
 
+@pytest.mark.parametrize("wt", [G.I32, G.F32])
+def test_tuner_then_auto_solves(wt):
+    """adds_tune picks an engine and knobs on sample sources; later solves
+    with default options use them and still match the oracle."""
+    if wt == G.I32:
+        g = G.rmat(15, 16, seed=21, w_hi=10000)
+    else:
+        g = G.grid(128, 96, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=22)
+    deg = np.diff(g.row.astype(np.int64))
+    srcs = [int(x) for x in np.random.default_rng(5).choice(np.flatnonzero(deg > 0), 3,
+                                                             replace=False)]
+    dg = A.Graph.from_csr(g)
+    try:
+        best, ms = dg.tune(srcs[:2])
+        assert best.engine in (ASYNC, PHASE) and ms > 0 and best.delta_shift >= 0
+        for s in srcs:
+            d, st = dg.sssp(s, A.default_opts(**OPTS))
+            assert st["engine"] == best.engine
+            ref, _ = O.dijkstra(g, s)
+            assert np.array_equal(d, ref), s
+    finally:
+        dg.close()
+
+
 @pytest.mark.parametrize("lh", [0, 1, 2])
 @pytest.mark.parametrize("solo", [0, 64])
 @pytest.mark.parametrize("shift", [6, 10])
