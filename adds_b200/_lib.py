@@ -166,6 +166,7 @@ SIGNATURES = [
     ("adds_sssp_backward", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.POINTER(Opts)]),
     ("adds_diag_relax_pass", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
+    ("adds_diag_wait_timeout", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("adds_graph_trace", C.c_int, [C.c_void_p, C.c_uint32]),
     ("adds_graph_trace_read", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32,
                                         C.POINTER(C.c_uint64)]),

@@ -1639,7 +1639,11 @@ extern "C" int adds_batch_sync(adds_batch *b, adds_stats *stats) {
   CK(cudaStreamSynchronize(b->stream));
   const bool phase = b->kn.engine == ADDS_ENGINE_PHASE;
   int rc = phase ? phase_status(b->peng) : engine_status(b->eng);
-  if (rc) return rc;
+  if (rc) {
+    /* reported: the next launch starts from a clean engine */
+    if (phase) ph_engine_reset(b->peng, b->stream); else engine_full_reset(b->eng, b->stream);
+    return rc;
+  }
   if (stats) {
     memset(stats, 0, sizeof *stats);
     float ms = 0, kms = 0;
@@ -1794,6 +1798,18 @@ static double time_solves(adds_graph *g, const uint32_t *srcs, uint32_t ns, cons
   cudaEventDestroy(a);
   cudaEventDestroy(z);
   return best;
+}
+
+extern "C" int adds_diag_wait_timeout(int device, int timeout_ms, double *waited_ms) {
+  if (timeout_ms <= 0 || timeout_ms > 10000) return ADDS_ERR_INVALID;
+  unsigned err = 0, where = 0;
+  float ms = 0.f;
+  if (ph_diag_wait(device, (unsigned)timeout_ms, &err, &where, &ms) != 0)
+    return cuda_fail(cudaGetLastError(), "diagnostic wait");
+  if (waited_ms) *waited_ms = ms;
+  if (err == 0u) return ADDS_OK;
+  snprintf(g_last_err, sizeof g_last_err, "device error %u at wait site %u", err, where);
+  return err == PH_ERR_TIMEOUT ? ADDS_ERR_DEVICE_TIMEOUT : ADDS_ERR_CUDA;
 }
 
 extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_opts *best,

@@ -1306,7 +1306,56 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
   return cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB>, P);
 }
 
+/* Failure-detection check: thread 0 waits, through the same bounded Waiter
+ * as the group barrier, for a flag that nothing sets.  The deadline runs out,
+ * the error word records a timeout at the barrier's wait site, and the
+ * kernel returns with the context intact.  An iteration cap bounds the loop
+ * even if the timer were not to advance. */
+__global__ void diag_wait_kernel(const unsigned *flag, PhGlobal *g,
+                                 unsigned long long timeout_ns) {
+  if (threadIdx.x != 0u || blockIdx.x != 0u) return;
+  Waiter w{gtimer() + timeout_ns, 0};
+  for (unsigned long long it = 0; ld_acq32(flag) == 0u; ++it) {
+    if (it > (1ull << 24)) {
+      raise_err(g, PH_ERR_TIMEOUT, W_BARRIER);
+      return;
+    }
+    if (!w.spin(g, W_BARRIER, 1024)) return;
+  }
+}
+
 }  // namespace adds_phase
+
+int ph_diag_wait(int device, unsigned timeout_ms, unsigned *err, unsigned *where,
+                 float *waited_ms) {
+  if (cudaSetDevice(device) != cudaSuccess) return -5;
+  PhGlobal *g = nullptr;
+  unsigned *flag = nullptr;
+  cudaEvent_t a = nullptr, z = nullptr;
+  int rc = -5;
+  if (cudaMalloc(&g, sizeof(PhGlobal)) == cudaSuccess &&
+      cudaMalloc(&flag, sizeof(unsigned)) == cudaSuccess &&
+      cudaMemset(g, 0, sizeof(PhGlobal)) == cudaSuccess &&
+      cudaMemset(flag, 0, sizeof(unsigned)) == cudaSuccess &&
+      cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&z) == cudaSuccess) {
+    cudaEventRecord(a, 0);
+    adds_phase::diag_wait_kernel<<<1, 32>>>(flag, g, (unsigned long long)timeout_ms * 1000000ull);
+    cudaEventRecord(z, 0);
+    PhGlobal h;
+    if (cudaGetLastError() == cudaSuccess && cudaEventSynchronize(z) == cudaSuccess &&
+        cudaMemcpy(&h, g, sizeof(PhGlobal), cudaMemcpyDeviceToHost) == cudaSuccess) {
+      *err = h.err;
+      *where = h.err_where;
+      cudaEventElapsedTime(waited_ms, a, z);
+      rc = 0;
+    }
+  }
+  if (a) cudaEventDestroy(a);
+  if (z) cudaEventDestroy(z);
+  if (flag) cudaFree(flag);
+  if (g) cudaFree(g);
+  return rc;
+}
 
 /* Kernel variants: (threads per CTA, CTAs per SM the registers are sized
  * for).  variant 0: 256 x 4, 1: 512 x 2, 2: 1024 x 1, 5: 128 x 8 (64
@@ -1341,6 +1390,7 @@ cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st) {
 
 /* ======================================================================== */
 /* host side                                                                  */
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -1528,7 +1578,14 @@ int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return -5;
   const unsigned fl = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
-  if (cudaMemsetAsync(E.g, 0, sizeof(PhGlobal), st) != cudaSuccess) return -5;
+  /* statistics and the batch counter start at zero; the error word is kept,
+   * so after a failed solve the ones queued behind it exit at once and the
+   * failure reaches the host at the next synchronisation (the host resets
+   * the engine once it has reported the error) */
+  const size_t keep = offsetof(PhGlobal, next_q);
+  if (cudaMemsetAsync(reinterpret_cast<char *>(E.g) + keep, 0, sizeof(PhGlobal) - keep, st) !=
+      cudaSuccess)
+    return -5;
   if (k0 && cudaEventRecordWithFlags(k0, st, fl) != cudaSuccess) return -5;
   if (adds_phase_launch(P, (int)E.variant, st) != cudaSuccess) return -5;
   if (k1 && cudaEventRecordWithFlags(k1, st, fl) != cudaSuccess) return -5;

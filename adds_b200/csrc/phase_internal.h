@@ -231,6 +231,10 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
                     const PhKnobs &k, unsigned grow, cudaStream_t st);
 void ph_engine_free(PhEngine &E);
 int ph_engine_reset(PhEngine &E, cudaStream_t st);
+/* bounded wait on a flag nothing sets (failure-detection check): the error
+ * word and wait site it left, and how long the kernel ran */
+int ph_diag_wait(int device, unsigned timeout_ms, unsigned *err, unsigned *where,
+                 float *waited_ms);
 int ph_engine_upload(PhEngine &E, cudaStream_t st);
 int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P);
 int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent_t k0,

@@ -328,6 +328,13 @@ int adds_graph_trace_read(adds_graph *g, adds_phase_trace *out, uint32_t cap,
  * edge without the gather.  [1] bounds any push-based relaxation schedule on
  * this GPU.  Allocates (the pass needs 4 B per edge and two distance arrays). */
 int adds_diag_relax_pass(adds_graph *g, uint32_t src, double ms_out[4]);
+/* Failure-detection check, no counterpart in the reference (whose worklist
+ * traps with a device assert, ads_int/wl.h:614-619): one thread waits, through
+ * the engine's bounded barrier wait, for a flag that nothing sets.  After
+ * timeout_ms (1..10000) the wait gives up and the call returns
+ * ADDS_ERR_DEVICE_TIMEOUT with the GPU context intact; waited_ms (may be
+ * NULL) receives the kernel's duration. */
+int adds_diag_wait_timeout(int device, int timeout_ms, double *waited_ms);
 
 /* ---- autotuner ---------------------------------------------------------- */
 /* Times candidate settings on the sample sources and stores the fastest in

@@ -74,6 +74,8 @@ def test_invalid_arguments_return_codes():
     assert lib.adds_graph_from_csr(0, 0, None, None, None, 0, 0, C.byref(h)) == -1
     assert lib.adds_sssp(None, 0, None, None, None) == -1
     assert lib.adds_sssp_sources(None, None, 0, None, None, None) == -1
+    assert lib.adds_diag_wait_timeout(0, 0, None) == -1
+    assert lib.adds_diag_wait_timeout(0, 20000, None) == -1
     assert lib.adds_batch_create(None, None, 0, None, C.byref(h)) == -1
     assert lib.adds_tune(None, None, 0, None, None) == -1
     assert lib.adds_write_dist_text(None, 0, None, 0) == -1
