@@ -17,8 +17,8 @@
  *     order, computed by the last child to finish ("last arriver
  *     continues" up the tree): no float atomics, fixed summation order;
  *   - grad[e] sums the queries of a graph in query order.
- * The CPU oracle (oracle/adjoint_ref.c) follows the same orders, so the
- * gradient is bit-exact against it.
+ * The CPU oracle's adjoint (oracle_adjoint in oracle/oracle.c) follows the
+ * same orders, so the gradient is bit-exact against it.
  */
 #include <cuda_runtime.h>
 #include <string.h>

@@ -23,6 +23,12 @@
  * there, so each call first clears the state that must start at zero.  Calls
  * whose work overlaps on the GPU (two streams, or two host threads) share
  * that memory and race; issue them one after another.
+ *
+ * The caller's arrays are validated on the device before the solver reads
+ * them (row offsets, dst < n, weights), as the allocating path validates a
+ * graph when it builds it; a failed check returns ADDS_ERR_FORMAT and the
+ * solver never touches the arrays.  The bucket width is derived on the
+ * device from a weight sample, so a call waits for the GPU once, at its end.
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -67,19 +73,74 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[ADDS_NOALLOC_SC
 
 namespace {
 
-__global__ void na_setup(PhQuery *qd, PhQuery desc) { *qd = desc; }
+/* Failed-check bits of the validation word (the allocating path checks the
+ * same properties when it builds a graph, api.cu k_check_rows /
+ * k_pack_edges). */
+enum : unsigned { BAD_DST = 1u, BAD_FLOAT_W = 2u, BAD_INT_W = 4u, BAD_ROWS = 8u };
 
-/* mean of evenly spaced weights (the delta heuristic needs the scale) */
-__global__ void na_sample(const uint2 *edges, unsigned long long m, int is_float, unsigned ns,
-                          double *out) {
+/* Validation of the caller's arrays, and the mean of evenly spaced weights
+ * (the bucket width needs it).  Rows: row[0] == 0, row[n] == m, offsets
+ * non-decreasing; edges: dst < n, int weights in [0, INT32_MAX], float
+ * weights not negative and not NaN (-0.0 is accepted: it sums like +0.0).
+ * Nothing is read past row[n] or edges[m-1]. */
+__global__ void na_check(const unsigned *row, const uint2 *edges, unsigned n,
+                         unsigned long long m, int is_float, unsigned ns, double *wsum,
+                         unsigned *bad) {
+  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned b = 0u;
+  if (tid == 0 && (row[0] != 0u || (unsigned long long)row[n] != m)) b |= BAD_ROWS;
+  for (unsigned long long v = tid; v < n; v += nth) {
+    const unsigned a = row[v], e = row[v + 1];
+    if (e < a || (unsigned long long)e > m) b |= BAD_ROWS;
+  }
+  for (unsigned long long i = tid; i < m; i += nth) {
+    const uint2 x = edges[i];
+    if (x.x >= n) b |= BAD_DST;
+    if (is_float) {
+      if (x.y != 0x80000000u && x.y > 0x7F800000u) b |= BAD_FLOAT_W;
+    } else if (x.y > 0x7FFFFFFFu) {
+      b |= BAD_INT_W;
+    }
+  }
   double acc = 0;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+  for (unsigned long long i = tid; i < ns; i += nth) {
     const unsigned long long e = (unsigned long long)((double)i * (double)m / (double)ns);
     const unsigned x = edges[e < m ? e : m - 1].y;
-    acc += is_float ? (double)__uint_as_float(x) : (double)x;
+    acc += is_float ? (double)__uint_as_float(x & 0x7FFFFFFFu) : (double)x;
   }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
-  if ((threadIdx.x & 31u) == 0u) atomicAdd(out, acc);
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+    b |= __shfl_down_sync(0xFFFFFFFFu, b, o);
+  }
+  if ((threadIdx.x & 31u) == 0u) {
+    if (acc != 0.0) atomicAdd(wsum, acc);
+    if (b) atomicOr(bad, b);
+  }
+}
+
+/* The solve's descriptor, with the bucket width worked out here from the
+ * sampled mean weight so the host never waits for it: delta ~ 4 x mean
+ * weight / mean degree key units (the allocating path's starting point,
+ * api.cu auto_shift), shift = nearest integer to log2(delta) in [0, 31];
+ * float keys are dist * 2^16 / mean weight (api.cu auto_scale).  Arrays
+ * that failed validation set the error word instead, and the solver exits
+ * at its first decision without touching them. */
+__global__ void na_setup(PhQuery *qd, PhQuery desc, int is_float, const double *wsum,
+                         unsigned ns, const unsigned *bad, PhGlobal *g) {
+  const double avg_w = ns ? *wsum / ns : 1.0;
+  const double deg = (double)desc.m / desc.n > 1.0 ? (double)desc.m / desc.n : 1.0;
+  const double aw = avg_w > 1e-30 ? avg_w : 1.0;
+  const double dk = is_float ? 4.0 * 65536.0 / deg : 4.0 * (avg_w > 1.0 ? avg_w : 1.0) / deg;
+  unsigned shift = 0;
+  while (shift < 31u && (double)(1ull << shift) * 1.4142135623730951 <= dk) ++shift;
+  desc.shift = shift;
+  desc.scale = (float)(65536.0 / aw);
+  *qd = desc;
+  if (*bad != 0u) {
+    g->err = PH_ERR_INPUT;
+    g->err_where = *bad;
+  }
 }
 
 struct DevState {
@@ -139,38 +200,26 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   PhGroup *grp = (PhGroup *)(B + kOffGrp);
   PhQuery *qd = (PhQuery *)(B + kOffQd);
   double *wsum = (double *)(B + kOffSum);
+  unsigned *bad = (unsigned *)(B + kOffSum + 8);
   unsigned long long *pt = (unsigned long long *)(B + kOffPt);
   PhHub *hub = (PhHub *)(B + kOffHub);
   unsigned *hub_seq = (unsigned *)(B + kOffHubSeq);
   unsigned long long *pool = (unsigned long long *)(B + kOffPool);
 
-  /* the delta heuristic of the allocating path: bucket width from the mean
-   * weight and the mean degree */
-  const unsigned ns = (unsigned)(m < (1u << 16) ? m : (1u << 16));
-  double sum = 0.0;
-  NA_CK(cudaMemsetAsync(wsum, 0, 8, st));
-  if (ns) {
-    na_sample<<<64, 256, 0, st>>>((const uint2 *)edges, m, flt, ns, wsum);
-    NA_CK(cudaGetLastError());
-    NA_CK(cudaMemcpyAsync(&sum, wsum, 8, cudaMemcpyDeviceToHost, st));
-    NA_CK(cudaStreamSynchronize(st));
-  }
-  const double avg_w = ns ? sum / ns : 1.0;
-  const double deg = (double)m / n > 1.0 ? (double)m / n : 1.0;
-  const double aw = avg_w > 1e-30 ? avg_w : 1.0;
-  const float scale = (float)(65536.0 / aw);
-  const double dk = flt ? 8.0 * 65536.0 / deg : 8.0 * (avg_w > 1.0 ? avg_w : 1.0) / deg;
-  int shift = 0;
-  while (shift < 31 && (double)(1u << (shift + 1)) <= dk * 1.41421356) ++shift;
-
   /* clear the state that must start at zero (the array keeps the previous
    * call's contents): group barrier and lists, statistics and error word,
-   * page-table tags, split-row record sequence words.  Pool pages are always
-   * written before they are read. */
+   * weight sum and validation word, page-table tags, split-row record
+   * sequence words.  Pool pages are always written before they are read. */
   NA_CK(cudaMemsetAsync(g, 0, sizeof(PhGlobal), st));
   NA_CK(cudaMemsetAsync(grp, 0, sizeof(PhGroup), st));
+  NA_CK(cudaMemsetAsync(wsum, 0, 16, st));
   NA_CK(cudaMemsetAsync(pt, 0xFF, kPtBytes, st));
   NA_CK(cudaMemsetAsync(hub_seq, 0, (size_t)kHubCap * 4, st));
+  /* the caller's arrays are checked on the device before the solver reads
+   * them, and the bucket width is worked out there too */
+  const unsigned ns = (unsigned)(m < (1u << 16) ? m : (1u << 16));
+  na_check<<<2 * 148, 256, 0, st>>>(row_start, (const uint2 *)edges, n, m, flt, ns, wsum, bad);
+  NA_CK(cudaGetLastError());
   PhQuery desc;
   memset(&desc, 0, sizeof desc);
   desc.row = row_start;
@@ -179,10 +228,8 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   desc.dist = dist;
   desc.n = n;
   desc.src = src;
-  desc.scale = scale;
-  desc.shift = (unsigned)shift;
   desc.m = m;
-  na_setup<<<1, 1, 0, st>>>(qd, desc);
+  na_setup<<<1, 1, 0, st>>>(qd, desc, flt, wsum, ns, bad, g);
   NA_CK(cudaGetLastError());
 
   PhParams P;
@@ -215,7 +262,15 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   NA_CK(cudaStreamSynchronize(st));
 #undef NA_CK
   if (err[0] == 0u) return ADDS_OK;
-  char msg[120];
+  char msg[160];
+  if (err[0] == PH_ERR_INPUT) {
+    snprintf(msg, sizeof msg, "invalid graph arrays:%s%s%s%s",
+             (err[1] & BAD_ROWS) ? " row offsets" : "", (err[1] & BAD_DST) ? " dst >= n" : "",
+             (err[1] & BAD_FLOAT_W) ? " negative or NaN float weight" : "",
+             (err[1] & BAD_INT_W) ? " negative int weight" : "");
+    adds_set_last_error(msg);
+    return ADDS_ERR_FORMAT;
+  }
   snprintf(msg, sizeof msg, "device error %u at wait site %u", err[0], err[1]);
   adds_set_last_error(msg);
   if (err[0] == PH_ERR_OVERFLOW || err[0] == PH_ERR_HUB_OVERFLOW) return ADDS_ERR_WL_OVERFLOW;

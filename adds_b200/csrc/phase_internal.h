@@ -44,6 +44,8 @@
 #define PH_ERR_OVERFLOW 2u
 #define PH_ERR_HUB_OVERFLOW 3u
 #define PH_ERR_MAPPING 4u
+#define PH_ERR_INPUT 5u    /* caller's arrays failed validation (no-alloc path);
+                              err_where holds the failed checks            */
 
 /* Read-only per-query descriptor. */
 struct PhQuery {

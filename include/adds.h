@@ -280,7 +280,12 @@ int adds_sssp_backward(adds_graph *g, uint32_t ns, const uint32_t *srcs,
  *   row_start: n+1 u32 row offsets; edges: 2*m u32 words, {dst, weight bits}
  *   per edge in CSR order; dist: n words, overwritten (same INF values as
  *   adds_sssp); all three on the current device.  stream: cudaStream_t or
- *   NULL.  Returns after the solve has finished on that stream.
+ *   NULL.  The call waits once for that stream, at its end, and returns
+ *   after the solve has finished.
+ * The arrays are checked on the device before the solver reads them (row
+ * offsets start at 0, never decrease and end at m; dst < n; weights not
+ * negative and, for floats, not NaN; -0.0f is accepted and sums like
+ * +0.0f); a failed check returns ADDS_ERR_FORMAT with dist untouched.
  * Graphs above ADDS_NOALLOC_MAX_N vertices or ADDS_NOALLOC_MAX_M edges are
  * rejected (ADDS_ERR_UNSUPPORTED); a graph within the limits whose queues
  * outgrow the fixed pool reports ADDS_ERR_WL_OVERFLOW.  The first call on a

@@ -6,6 +6,7 @@ module; the product never does.  See oracle.c for what it restates.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import os
 import subprocess
 
@@ -37,8 +38,71 @@ def lib():
         L.oracle_delta_step.restype = C.c_int
         L.oracle_adjoint.argtypes = [u32, u64, vp, vp, vp, u32, vp, vp, vp, vp, vp]
         L.oracle_adjoint.restype = C.c_int
+        dbl = C.c_double
+        L.oracle_gen_rmat.argtypes = [C.c_int, C.c_int, dbl, dbl, dbl, C.c_int, dbl, dbl, u64,
+                                      C.c_int, vp, vp, vp, u64, C.POINTER(u64)]
+        L.oracle_gen_rmat.restype = C.c_int
+        L.oracle_gen_grid.argtypes = [u32, u32, dbl, C.c_int, C.c_int, dbl, dbl, u64, C.c_int, vp,
+                                      vp, vp, u64, C.POINTER(u64)]
+        L.oracle_gen_grid.restype = C.c_int
         _lib = L
     return _lib
+
+
+@dataclasses.dataclass
+class HostCSR:
+    """CSR arrays on the host (row uint64[n+1], dst/w uint32[m], w holding
+    int32 values or float32 bits per wtype); the layout of
+    adds_b200.graphs.CSR, without importing the product package."""
+    n: int
+    row: np.ndarray
+    dst: np.ndarray
+    w: np.ndarray
+    wtype: int
+
+    @property
+    def m(self) -> int:
+        return int(self.dst.shape[0])
+
+    def weights(self):
+        return self.w.view(np.float32) if self.wtype == 1 else self.w.view(np.int32)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, wtype: int = 0,
+             w_lo=1.0, w_hi=1000.0, seed: int = 1, threads: int | None = None) -> HostCSR:
+    """The seeded R-MAT generator (gen.c), multithreaded on the host."""
+    threads = threads or os.cpu_count() or 1
+    n = 1 << scale
+    cap = edge_factor * n
+    row = np.empty(n + 1, dtype=np.uint64)
+    dst = np.empty(cap, dtype=np.uint32)
+    w = np.empty(cap, dtype=np.uint32)
+    m = C.c_uint64()
+    rc = lib().oracle_gen_rmat(scale, edge_factor, a, b, c, wtype, float(w_lo), float(w_hi), seed,
+                               threads, row.ctypes.data, dst.ctypes.data, w.ctypes.data, cap,
+                               C.byref(m))
+    if rc:
+        raise RuntimeError(f"oracle_gen_rmat failed ({rc})")
+    return HostCSR(n, row, dst[:m.value], w[:m.value], wtype)
+
+
+def gen_grid(side_x: int, side_y: int, shortcut_frac=0.0, radius=8, wtype: int = 1, w_lo=1.0,
+             w_hi=100.0, seed: int = 1, threads: int | None = None) -> HostCSR:
+    """The seeded grid-with-shortcuts generator (gen.c), on the host."""
+    threads = threads or os.cpu_count() or 1
+    n = side_x * side_y
+    egrid = 2 * (side_x - 1) * side_y + 2 * side_x * (side_y - 1)
+    cap = 4 * n + 2 * int(shortcut_frac * egrid + 0.5) + 2
+    row = np.empty(n + 1, dtype=np.uint64)
+    dst = np.empty(cap, dtype=np.uint32)
+    w = np.empty(cap, dtype=np.uint32)
+    m = C.c_uint64()
+    rc = lib().oracle_gen_grid(side_x, side_y, float(shortcut_frac), radius, wtype, float(w_lo),
+                               float(w_hi), seed, threads, row.ctypes.data, dst.ctypes.data,
+                               w.ctypes.data, cap, C.byref(m))
+    if rc:
+        raise RuntimeError(f"oracle_gen_grid failed ({rc})")
+    return HostCSR(n, row, dst[:m.value], w[:m.value], wtype)
 
 
 def _arr(a, dt):

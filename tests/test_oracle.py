@@ -211,3 +211,25 @@ def test_oracle_pinned_to_reference_output(name):
     else:
         text = gzip.decompress(z["text_gz"].tobytes()).decode()
         assert G.dist_text(d, G.F32) == text
+
+
+@pytest.mark.parametrize("kind", ["rmat_int", "rmat_float", "grid_float", "plain_grid"])
+def test_host_generator_matches_numpy_twin(kind):
+    """oracle/gen.c (the reference arm's graph builder) produces the CSR of
+    adds_b200/graphs.py (and so of the GPU generator) bit for bit."""
+    if kind == "rmat_int":
+        a = O.gen_rmat(13, 16, wtype=0, w_lo=1, w_hi=10000, seed=24, threads=3)
+        b = G.rmat(13, 16, wtype=0, w_lo=1, w_hi=10000, seed=24)
+    elif kind == "rmat_float":
+        a = O.gen_rmat(11, 16, wtype=1, w_lo=0.0, w_hi=1.0, seed=26, threads=4)
+        b = G.rmat(11, 16, wtype=1, w_lo=0.0, w_hi=1.0, seed=26)
+    elif kind == "grid_float":
+        a = O.gen_grid(131, 77, 0.02, 8, wtype=1, w_lo=1.0, w_hi=100.0, seed=4096, threads=5)
+        b = G.grid(131, 77, 0.02, 8, wtype=1, w_lo=1.0, w_hi=100.0, seed=4096)
+    else:
+        a = O.gen_grid(40, 33, 0.0, 8, wtype=1, w_lo=1.0, w_hi=2.0, seed=9, threads=2)
+        b = G.grid(40, 33, 0.0, 8, wtype=1, w_lo=1.0, w_hi=2.0, seed=9)
+    assert a.n == b.n and a.m == b.m
+    assert np.array_equal(a.row, b.row)
+    assert np.array_equal(a.dst, b.dst)
+    assert np.array_equal(a.w, b.w)

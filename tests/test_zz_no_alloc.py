@@ -7,8 +7,10 @@ synchronisations).  It takes device arrays the caller owns and works in a
 fixed device array inside the library.  This test calls it through the C
 ABI, twice in a row per graph (the second call must not depend on what the
 first left in the shared array), and requires distances bit-identical to
-the allocating entry point's, the same tolerance as every other distance
-test here.  It lives in its own file so that it is collected last.
+the allocating entry point's and to the CPU oracle's, the same tolerance as
+every other distance test here.  Arrays with a defect are refused before
+the solver reads them.  It lives in its own file so that it is collected
+last.
 """
 import ctypes as C
 
@@ -18,6 +20,7 @@ import pytest
 import adds_b200 as A
 from adds_b200 import _lib as L
 from adds_b200 import graphs as G
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -57,8 +60,44 @@ def test_noalloc_matches_allocating_entry_point(kind):
             want, _ = dg.sssp(s, A.default_opts(timeout_ms=10000))
             got = _noalloc(g, row, edges, s)
             assert np.array_equal(got, want), f"source {s}"
+            ref, _ = O.dijkstra(g, s)  # and the CPU oracle directly
+            assert np.array_equal(got, ref), f"source {s} vs oracle"
     finally:
         dg.close()
+
+
+def _corrupt(kind):
+    """A small graph with one defect made on the host."""
+    g = G.rmat(10, 8, seed=33, w_hi=1000)
+    row, dst, w = g.row.copy(), g.dst.copy(), g.w.copy()
+    if kind == "dst":
+        dst[g.m // 2] = g.n + 5
+    elif kind == "rows":
+        row[g.n // 2] = row[g.n // 2 + 1] + 1  # offsets decrease
+    elif kind == "int_weight":
+        w[7] = np.uint32(0x80000001)  # negative as int32
+    return G.CSR(g.n, row, dst, w, g.wtype)
+
+
+@pytest.mark.parametrize("kind", ["dst", "rows", "int_weight"])
+def test_noalloc_rejects_invalid_arrays(kind):
+    """Arrays that would send the solver outside the caller's buffers are
+    refused before it reads them, and the output is left untouched."""
+    import torch
+    g = _corrupt(kind)
+    row, edges = _device_csr(g)
+    out = torch.full((g.n,), 12345, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    rc = L.lib().adds_sssp_noalloc(g.n, g.m, row.data_ptr(), edges.data_ptr(), g.wtype, 0,
+                                   out.data_ptr(), None)
+    assert rc == -3  # ADDS_ERR_FORMAT
+    assert b"invalid graph arrays" in L.lib().adds_last_cuda_error()
+    assert bool((out == 12345).all())
+    # the shared array is usable again at once
+    good = G.rmat(10, 8, seed=34, w_hi=1000)
+    r2, e2 = _device_csr(good)
+    ref, _ = O.dijkstra(good, 3)
+    assert np.array_equal(_noalloc(good, r2, e2, 3), ref)
 
 
 def test_noalloc_rejects_graphs_over_the_limit():
