@@ -22,6 +22,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "../../include/adds.h"
@@ -482,11 +483,23 @@ __global__ void k_check_rows(const unsigned *row, uint32_t n, uint64_t m, unsign
   unsigned md = 0;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const unsigned a = row[v], b = row[v + 1];
-    if (b < a || b > m) atomicOr(bad, 8u);
+    if (b < a || b > m || (v == 0 && a != 0u) || (v == n - 1 && b != m)) atomicOr(bad, 8u);
     else md = max(md, b - a);
   }
   for (int o = 16; o > 0; o >>= 1) md = max(md, __shfl_down_sync(0xFFFFFFFFu, md, o));
   if ((threadIdx.x & 31u) == 0u) atomicMax(maxdeg, md);
+}
+/* .gr row end offsets (u64) -> u32 row[i0 + 1 + i]; an offset above m (it
+ * would not fit the u32 CSR) is flagged, the order is checked later by
+ * k_check_rows */
+__global__ void k_rows_u64(const unsigned long long *ends, uint64_t cnt, uint64_t i0, uint64_t m,
+                           unsigned *row, unsigned *bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cnt;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long e = ends[i];
+    if (e > m) atomicOr(bad, 8u);
+    row[i0 + 1 + i] = (unsigned)(e > m ? m : e);
+  }
 }
 /* evenly spaced weight sample (profiler_kernel, ads_int/kernel.cu:153-183) */
 __global__ void k_sample_w(const uint2 *edges, uint64_t m, int is_float, unsigned ns, double *out) {
@@ -608,6 +621,139 @@ static int graph_upload(adds_graph *g, const unsigned *row_host_u32, const uint3
   return graph_finish(g);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Host -> device ingest through pinned staging.  Replaces the per-edge host
+ * loop of readFromGR (ads_int/csr_graph.cu:260-280) and the pageable
+ * cudaMemcpy calls of copy_to_gpu (csr_graph.cu:309-328): several host
+ * threads read the next piece (pread from the file, or memcpy from caller
+ * memory) into one of two pinned buffers while the GPU copies the other
+ * piece in and converts it (row offsets u64 -> u32, {dst, weight} packing
+ * and checks).  Nothing is parsed on the host. */
+struct HostSrc {
+  int fd = -1;                 /* pread from this file at off + byte offset ... */
+  uint64_t off = 0;
+  const char *mem = nullptr;   /* ... or copy from this address                */
+  bool present() const { return fd >= 0 || mem != nullptr; }
+};
+
+static bool host_fill(const HostSrc &s, void *out, uint64_t at, size_t bytes, int nth) {
+  if (bytes == 0) return true;
+  const size_t min_slice = (size_t)1 << 20;
+  int t = (int)std::min<size_t>((size_t)nth, (bytes + min_slice - 1) / min_slice);
+  if (t < 1) t = 1;
+  std::vector<char> ok((size_t)t, 1);
+  auto part = [&](int i) {
+    const size_t a = bytes * (size_t)i / (size_t)t, b = bytes * (size_t)(i + 1) / (size_t)t;
+    char *o = (char *)out + a;
+    if (s.mem) {
+      memcpy(o, s.mem + at + a, b - a);
+      return;
+    }
+    size_t done = 0;
+    while (done < b - a) {
+      const ssize_t r = pread(s.fd, o + done, b - a - done, (off_t)(s.off + at + a + done));
+      if (r <= 0) {
+        if (r < 0 && errno == EINTR) continue;
+        ok[(size_t)i] = 0;
+        return;
+      }
+      done += (size_t)r;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < t; ++i) th.emplace_back(part, i);
+  part(0);
+  for (auto &x : th) x.join();
+  for (char c : ok)
+    if (!c) return false;
+  return true;
+}
+
+/* rows: the n row END offsets as u64 (row[0] = 0 is implied); dst and w:
+ * m u32 words each (w absent = all-zero weights, as a .gr without edge
+ * data).  g->n and g->m are set.  Ends with graph_finish's checks. */
+static int graph_ingest(adds_graph *g, const HostSrc &rows, const HostSrc &dst, const HostSrc &w) {
+  const uint64_t n = g->n, m = g->m;
+  constexpr uint64_t CH = (uint64_t)1 << 22; /* words per piece: 16 MB of dst + 16 MB of w */
+  constexpr size_t BUF = (size_t)CH * 8;     /* bytes per staging buffer                   */
+  const int nth = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  CK(cudaMalloc(&g->row, (n + 1) * 4));
+  CK(cudaMalloc(&g->edges, (m + ADDS_EDGE_PAD) * sizeof(uint2)));
+  g->bytes = (n + 1) * 4 + m * sizeof(uint2);
+  CK(cudaMemsetAsync(g->row, 0, 4, g->stream));
+  CK(cudaMemsetAsync(g->edges + m, 0, ADDS_EDGE_PAD * sizeof(uint2), g->stream));
+  char *pin[2] = {nullptr, nullptr};
+  char *dev = nullptr;
+  unsigned *bad = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int rc = ADDS_OK;
+  auto cu = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && rc == ADDS_OK) rc = cuda_fail(e, what);
+    return rc == ADDS_OK;
+  };
+  if (cu(cudaHostAlloc((void **)&pin[0], BUF, cudaHostAllocDefault), "pinned staging") &&
+      cu(cudaHostAlloc((void **)&pin[1], BUF, cudaHostAllocDefault), "pinned staging") &&
+      cu(cudaMalloc(&dev, 2 * BUF), "device staging") && cu(cudaMalloc(&bad, 4), "flag") &&
+      cu(cudaMemsetAsync(bad, 0, 4, g->stream), "flag") &&
+      cu(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "event") &&
+      cu(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "event")) {
+    /* pieces: row ends in CH-entry pieces, then edges in CH-edge pieces */
+    const uint64_t nrp = (n + CH - 1) / CH, nep = (m + CH - 1) / CH;
+    for (uint64_t c = 0; c < nrp + nep && rc == ADDS_OK; ++c) {
+      const int k = (int)(c & 1);
+      if (c >= 2 && !cu(cudaEventSynchronize(ev[k]), "staging wait")) break;
+      char *p = pin[k], *d = dev + (size_t)k * BUF;
+      if (c < nrp) {
+        const uint64_t i0 = c * CH, cnt = std::min(CH, n - i0);
+        if (!host_fill(rows, p, i0 * 8, cnt * 8, nth)) {
+          rc = ADDS_ERR_IO;
+          break;
+        }
+        if (!cu(cudaMemcpyAsync(d, p, cnt * 8, cudaMemcpyHostToDevice, g->stream), "rows H2D") ||
+            !cu(cudaEventRecord(ev[k], g->stream), "event"))
+          break;
+        k_rows_u64<<<592, 256, 0, g->stream>>>((const unsigned long long *)d, cnt, i0, m, g->row,
+                                              bad);
+      } else {
+        const uint64_t i0 = (c - nrp) * CH, cnt = std::min(CH, m - i0);
+        if (!host_fill(dst, p, i0 * 4, cnt * 4, nth) ||
+            (w.present() && !host_fill(w, p + CH * 4, i0 * 4, cnt * 4, nth))) {
+          rc = ADDS_ERR_IO;
+          break;
+        }
+        if (!cu(cudaMemcpyAsync(d, p, cnt * 4, cudaMemcpyHostToDevice, g->stream), "dst H2D") ||
+            (w.present() && !cu(cudaMemcpyAsync(d + CH * 4, p + CH * 4, cnt * 4,
+                                                cudaMemcpyHostToDevice, g->stream), "w H2D")) ||
+            !cu(cudaEventRecord(ev[k], g->stream), "event"))
+          break;
+        k_pack_edges<<<592, 256, 0, g->stream>>>((const uint32_t *)d,
+                                                w.present() ? (const uint32_t *)(d + CH * 4)
+                                                            : nullptr,
+                                                cnt, (uint32_t)n, g->wt == ADDS_F32,
+                                                g->edges + i0, bad);
+      }
+      cu(cudaGetLastError(), "convert kernel");
+    }
+  }
+  unsigned hb = 0;
+  if (rc == ADDS_OK) {
+    cu(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, g->stream), "flag D2H");
+    cu(cudaStreamSynchronize(g->stream), "ingest");
+  } else {
+    cudaStreamSynchronize(g->stream);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (ev[k]) cudaEventDestroy(ev[k]);
+    if (pin[k]) cudaFreeHost(pin[k]);
+  }
+  if (dev) cudaFree(dev);
+  if (bad) cudaFree(bad);
+  if (rc) return rc;
+  if (hb & 9u) return ADDS_ERR_FORMAT; /* dst >= n, row offset > m */
+  if (hb & 6u) return ADDS_ERR_INVALID; /* negative or NaN weight */
+  return graph_finish(g);
+}
+
 extern "C" int adds_graph_from_csr(uint32_t n, uint64_t m, const uint64_t *row_start,
                                    const uint32_t *dst, const void *w, adds_wtype wt, int device,
                                    adds_graph **out) {
@@ -618,16 +764,26 @@ extern "C" int adds_graph_from_csr(uint32_t n, uint64_t m, const uint64_t *row_s
   int rc = set_device(device);
   if (rc) return rc;
   if (row_start[0] != 0 || row_start[n] != m) return ADDS_ERR_INVALID;
-  std::vector<unsigned> row(n + 1);
-  for (uint32_t v = 0; v <= n; ++v) {
-    if (v && row_start[v] < row_start[v - 1]) return ADDS_ERR_INVALID;
-    row[v] = (unsigned)row_start[v];
-  }
+  const bool dev_arrays = (dst && is_device_ptr(dst)) || (w && is_device_ptr(w));
   adds_graph *g = graph_new(device, wt);
   if (!g) return ADDS_ERR_CUDA;
   g->n = n;
   g->m = m;
-  rc = graph_upload(g, row.data(), dst, w);
+  if (!dev_arrays) {
+    /* host arrays: pinned, pipelined upload; the rows are checked on the GPU */
+    HostSrc rs, ds, ws;
+    rs.mem = (const char *)(row_start + 1);
+    ds.mem = (const char *)dst;
+    ws.mem = (const char *)w;
+    rc = graph_ingest(g, rs, ds, ws);
+  } else {
+    std::vector<unsigned> row(n + 1);
+    for (uint32_t v = 0; v <= n && !rc; ++v) {
+      if (v && row_start[v] < row_start[v - 1]) rc = ADDS_ERR_INVALID;
+      row[v] = (unsigned)row_start[v];
+    }
+    if (!rc) rc = graph_upload(g, row.data(), dst, w);
+  }
   if (rc) {
     adds_graph_free(g);
     return rc;
@@ -636,8 +792,10 @@ extern "C" int adds_graph_from_csr(uint32_t n, uint64_t m, const uint64_t *row_s
   return ADDS_OK;
 }
 
-/* .gr v1 reader (readFromGR, ads_int/csr_graph.cu:203-296): mmap, check the
- * header and the size, convert out_end[] to u32 row offsets, upload. */
+/* .gr v1 reader (readFromGR, ads_int/csr_graph.cu:203-296): the header and
+ * the file size are checked on the host; out_end[], dst[] and w[] are read
+ * by host threads straight into pinned staging buffers and converted and
+ * checked on the GPU (graph_ingest). */
 extern "C" int adds_graph_load_gr(const char *path, adds_wtype wt, int device, adds_graph **out) {
   if (!path || !out || (wt != ADDS_I32 && wt != ADDS_F32)) return ADDS_ERR_INVALID;
   *out = nullptr;
@@ -646,23 +804,19 @@ extern "C" int adds_graph_load_gr(const char *path, adds_wtype wt, int device, a
   const int fd = open(path, O_RDONLY);
   if (fd < 0) return ADDS_ERR_IO;
   struct stat sb;
+  uint64_t h[4];
   if (fstat(fd, &sb) != 0) {
     close(fd);
     return ADDS_ERR_IO;
   }
   const size_t len = (size_t)sb.st_size;
-  if (len < 32) {
+  if (len < 32 || pread(fd, h, 32, 0) != 32) {
     close(fd);
-    return ADDS_ERR_FORMAT;
+    return len < 32 ? ADDS_ERR_FORMAT : ADDS_ERR_IO;
   }
-  void *map = mmap(nullptr, len, PROT_READ, MAP_PRIVATE, fd, 0);
-  close(fd);
-  if (map == MAP_FAILED) return ADDS_ERR_IO;
-  const uint64_t *h = (const uint64_t *)map;
   const uint64_t version = h[0], esz = h[1], n64 = h[2], m64 = h[3];
   rc = ADDS_OK;
   adds_graph *g = nullptr;
-  std::vector<unsigned> row;
   if (version != 1 || (esz != 0 && esz != 4) || n64 == 0 || n64 >= 0x80000000ull ||
       m64 >= 0xFFFFFFFFull) {
     rc = ADDS_ERR_FORMAT;
@@ -671,31 +825,23 @@ extern "C" int adds_graph_load_gr(const char *path, adds_wtype wt, int device, a
     if (len < need) rc = ADDS_ERR_FORMAT;
   }
   if (!rc) {
-    const uint64_t *outidx = h + 4;
-    row.resize(n64 + 1);
-    row[0] = 0;
-    for (uint64_t v = 0; v < n64; ++v) {
-      const uint64_t e = outidx[v];
-      if (e < row[v] || e > m64) {
-        rc = ADDS_ERR_FORMAT;
-        break;
-      }
-      row[v + 1] = (unsigned)e;
-    }
-    if (!rc && row[n64] != m64) rc = ADDS_ERR_FORMAT;
-  }
-  if (!rc) {
-    const uint32_t *dst = (const uint32_t *)(h + 4 + n64);
-    const uint32_t *wv = esz ? dst + m64 + (m64 & 1) : nullptr;
     g = graph_new(device, wt);
     if (!g) rc = ADDS_ERR_CUDA;
     else {
       g->n = (uint32_t)n64;
       g->m = m64;
-      rc = graph_upload(g, row.data(), dst, wv);
+      HostSrc rs, ds, ws;
+      rs.fd = ds.fd = fd;
+      rs.off = 32;
+      ds.off = 32 + 8 * n64;
+      if (esz) {
+        ws.fd = fd;
+        ws.off = ds.off + 4 * m64 + ((m64 & 1) ? 4 : 0);
+      }
+      rc = graph_ingest(g, rs, ds, ws);
     }
   }
-  munmap(map, len);
+  close(fd);
   if (rc) {
     if (g) adds_graph_free(g);
     return rc;

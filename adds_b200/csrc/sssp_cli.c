@@ -3,7 +3,8 @@
  * (ads_int/sssp and ads_float/sssp; main at ads_int/kernel.cu:290-305,
  * options at ads_int/support.cu:11-76).
  *
- *   sssp_int   [-q] [-g gpu] [-o out|-] [-s start] [-r runs] [-d shift] [-t] graph.gr
+ *   sssp_int   [-q] [-g gpu] [-o out|-] [-b out.bin] [-s start] [-r runs] [-d shift] [-t]
+ *              graph.gr
  *   sssp_float [same]
  *
  * Same flags, same distance file ("<v> <d>" / "<v> INF"), same fd-3 record
@@ -11,8 +12,10 @@
  * (kernel.cu:215-216,282).  Like the reference, the int build averages 8
  * solves and counts popped vertices as work; the float build runs once and
  * counts scanned edges (ads_float/kernel.cu:59-60,225).  Extra flags:
- * -r runs, -d bucket shift, -t autotune before timing.  Errors print a
- * message and exit non-zero instead of asserting.
+ * -b raw distance words (n x 32-bit, little-endian; python -m
+ * adds_b200.verify compares two such files bit for bit), -r runs, -d
+ * bucket shift, -t autotune before timing.  Errors print a message and exit
+ * non-zero instead of asserting.
  */
 #include <errno.h>
 #include <stdint.h>
@@ -33,8 +36,8 @@
 
 static void usage(const char *prog) {
   fprintf(stderr,
-          "usage: %s [-q] [-g gpunum] [-o output-file] [-s startNode] [-r runs] [-d shift] [-t] "
-          "graph-file \n",
+          "usage: %s [-q] [-g gpunum] [-o output-file] [-b raw-output-file] [-s startNode] "
+          "[-r runs] [-d shift] [-t] graph-file \n",
           prog);
 }
 
@@ -46,17 +49,18 @@ static void die(const char *what, int rc) {
 int main(int argc, char **argv) {
   int quiet = 0, gpu = 0, runs = DEFAULT_RUNS, shift = -1, tune = 0;
   long start = 0;
-  const char *out = NULL;
+  const char *out = NULL, *out_bin = NULL;
   int c;
   if (argc == 1) {
     usage(argv[0]);
     return 1;
   }
-  while ((c = getopt(argc, argv, "g:qo:s:r:d:tl")) != -1) {
+  while ((c = getopt(argc, argv, "g:qo:b:s:r:d:tl")) != -1) {
     char *end = NULL;
     switch (c) {
       case 'q': quiet = 1; break;
       case 'o': out = optarg; break;
+      case 'b': out_bin = optarg; break;
       case 'g':
         errno = 0;
         gpu = (int)strtol(optarg, &end, 10);
@@ -122,13 +126,20 @@ int main(int argc, char **argv) {
     fprintf(d3, "%s %.3f %llu\n", base, total_ms / runs, total_work / (unsigned long long)runs);
     fflush(d3);
   }
-  if (out) {
+  if (out || out_bin) {
     uint32_t *dist = (uint32_t *)malloc((size_t)info.n * 4);
     if (!dist) die("malloc", ADDS_ERR_OOM);
     rc = adds_graph_last_dist(g, dist);
     if (rc) die("copy distances", rc);
-    rc = adds_write_dist_text(out, info.n, dist, WT);
-    if (rc) die("write output", rc);
+    if (out) {
+      rc = adds_write_dist_text(out, info.n, dist, WT);
+      if (rc) die("write output", rc);
+    }
+    if (out_bin) { /* raw 32-bit little-endian distance words, for bit checks */
+      FILE *f = fopen(out_bin, "wb");
+      if (!f || fwrite(dist, 4, info.n, f) != info.n || fclose(f) != 0)
+        die("write binary output", ADDS_ERR_IO);
+    }
     free(dist);
   }
   adds_graph_free(g);

@@ -20,7 +20,9 @@
 #      (ads_float/csr_graph.cu:343-345) -> sizeof(node_data_type), and
 #      output() prints the record through %f (ads_float/support.cu:93)
 #      -> prints .dist, INF being dist == FLT_MAX.
-# Outputs: oracle/_ref/ads_int_sssp, oracle/_ref/ads_float_sssp.
+# Outputs: oracle/_ref/ads_int_sssp, oracle/_ref/ads_float_sssp, and
+# oracle/_ref/ref_ingest (the int csr_graph.cu reader and upload under the
+# timing main oracle/ref_ingest_main.cu, for oracle/time_ingest.py).
 set -euo pipefail
 REF=${REF:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -48,6 +50,11 @@ for v in int float; do
   grep -q '#define MAX_TB 512' wl.h || { echo "MAX_TB patch did not apply" >&2; exit 3; }
   "$NVCC" kernel.cu support.cu csr_graph.cu -O3 -gencode arch=compute_100a,code=sm_100a \
     -rdc=true -lcudadevrt -w -o "$OUT/ads_${v}_sssp"
+  if [ "$v" = int ]; then
+    # the reference's own reader and upload (csr_graph.cu) under a timing main
+    "$NVCC" "$HERE/ref_ingest_main.cu" csr_graph.cu -I. -O3 \
+      -gencode arch=compute_100a,code=sm_100a -w -o "$OUT/ref_ingest"
+  fi
   cd - > /dev/null
 done
-echo "built: $OUT/ads_int_sssp $OUT/ads_float_sssp"
+echo "built: $OUT/ads_int_sssp $OUT/ads_float_sssp $OUT/ref_ingest"

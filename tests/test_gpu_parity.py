@@ -339,6 +339,41 @@ def test_cli_int_matches_reference_text(tmp_path):
     assert name == "r12.gr" and float(ms) > 0 and int(work) > 0
 
 
+def test_cli_float_text_and_raw_words_match_oracle(tmp_path):
+    """sssp_float as run_all.sh runs it: the "%d %f" text equals the
+    oracle's, the raw words (-b) equal the oracle's bit for bit, and the
+    checker (python -m adds_b200.verify) agrees; the fd-3 record counts
+    scanned edges, as the reference float build does."""
+    import os
+    import subprocess
+    import sys
+    g = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=44)
+    src = 40 * 96 + 48
+    d1, d2 = tmp_path / "ours", tmp_path / "oracle"
+    d1.mkdir()
+    d2.mkdir()
+    p = str(tmp_path / "g96.gr")
+    G.write_gr(p, g)
+    rec = str(tmp_path / "fd3.txt")
+    exe = os.path.join(os.path.dirname(A._lib.HERE), "adds_b200", "bin", "sssp_float")
+    cmd = f'"{exe}" -q -s {src} -o "{d1}/g96.gr" -b "{d1}/g96.bin" "{p}" 3>"{rec}"'
+    r = subprocess.run(["bash", "-c", cmd], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    ref, _ = O.dijkstra(g, src)
+    assert open(f"{d1}/g96.gr").read() == G.dist_text(ref, G.F32)
+    assert np.array_equal(np.fromfile(f"{d1}/g96.bin", dtype="<u4"), ref)
+    name, ms, work = open(rec).read().split()
+    assert name == "g96.gr" and float(ms) > 0 and int(work) >= g.m // 2
+    (d2 / "g96.gr").write_text(G.dist_text(ref, G.F32))
+    ref.astype("<u4").tofile(str(d2 / "g96.bin"))
+    lst = tmp_path / "list"
+    lst.write_text(f"g96.gr\t{src}\ng96.bin\t{src}\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    v = subprocess.run([sys.executable, "-m", "adds_b200.verify", f"{d1}/", f"{d2}/", str(lst),
+                        "--float"], capture_output=True, text=True, cwd=root, timeout=120)
+    assert v.returncode == 0 and "all results match!!!" in v.stdout, v.stdout
+
+
 @pytest.mark.parametrize("name", ["ref_rmat16_int", "ref_rmat12_int", "ref_grid96_float"])
 def test_engine_matches_reference_adds_output(name):
     """The engine against what the reference ADDS binary itself printed
