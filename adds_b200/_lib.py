@@ -59,7 +59,8 @@ class Opts(C.Structure):
         ("group_ctas", C.c_int32),
         ("solo_max", C.c_int32),
         ("near_far", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("dense_scan", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

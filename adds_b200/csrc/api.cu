@@ -267,7 +267,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
-  int engine, variant, group_ctas, solo_max, near_far; /* phase engine */
+  int engine, variant, group_ctas, solo_max, near_far, dense_scan; /* phase engine */
   unsigned long long timeout_ns;
 };
 
@@ -291,6 +291,7 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.adapt = k.adapt > 0 ? 1u : 0u;
   p.lh_adapt = k.light_heavy == 2 ? 1u : 0u;
   p.near_far = k.near_far ? 1u : 0u;
+  p.dense_shift = (k.dense_scan > 0 && !k.near_far) ? (unsigned)std::min(k.dense_scan, 31) : 0u;
   p.timeout_ns = k.timeout_ns;
   return p;
 }
@@ -388,6 +389,7 @@ struct adds_graph {
   unsigned *row = nullptr;
   uint2 *edges = nullptr;
   unsigned *dist = nullptr;
+  unsigned *settled = nullptr; /* phase engine settled filter, ceil(n/32) words */
   uint2 *sedges = nullptr;     /* rows sorted by weight (light edges first)   */
   unsigned *split = nullptr;   /* light-edge count per row for split_thr      */
   unsigned split_thr = 0;
@@ -533,6 +535,8 @@ static int graph_finish(adds_graph *g) {
   g->avg_w = ns ? sw / ns : 1.0;
   CK(cudaMalloc(&g->dist, ((size_t)g->n ? g->n : 1) * 4));
   g->bytes += (size_t)g->n * 4;
+  CK(cudaMalloc(&g->settled, (((size_t)g->n + 31) / 32) * 4));
+  g->bytes += (((size_t)g->n + 31) / 32) * 4;
   CK(cudaEventCreate(&g->ev0));
   CK(cudaEventCreate(&g->ev1));
   return ADDS_OK;
@@ -560,6 +564,7 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->row) cudaFree(g->row);
   if (g->edges) cudaFree(g->edges);
   if (g->dist) cudaFree(g->dist);
+  if (g->settled) cudaFree(g->settled);
   if (g->sedges) cudaFree(g->sedges);
   if (g->split) cudaFree(g->split);
   if (g->aux) cudaFree(g->aux);
@@ -1019,6 +1024,9 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   }
   k->group_ctas = o->group_ctas > 0 ? o->group_ctas : (t->group_ctas > 0 ? t->group_ctas : 0);
   k->solo_max = o->solo_max >= 0 ? o->solo_max : (t->solo_max >= 0 ? t->solo_max : 1024);
+  /* dense bucket slots: explicit > tuned > 6 (a slot holding more than n/64
+   * pushes is cheaper to collect with one pass over the distances) */
+  k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : 6);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -1170,13 +1178,15 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.edges = edges;
   q.split = split;
   q.dist = g->dist;
+  q.settled = g->settled;
   q.n = g->n;
   q.src = 0;
   q.scale = scale;
   q.shift = (unsigned)shift;
   q.m = g->m;
   PhEngine &E = g->peng;
-  if (E.nq == 1 && E.variant == (unsigned)k.variant && ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
+  if (E.nq == 1 && E.variant == (unsigned)k.variant && E.req_group == k.group_ctas &&
+      ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
     PhQuery &h = E.qs_host[0];
     if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)
       return ADDS_OK;
@@ -1556,6 +1566,7 @@ struct adds_batch {
   std::vector<adds_graph *> ugraph; /* distinct graphs, first-use order */
   std::vector<unsigned> qgid;
   unsigned *dist_all = nullptr;
+  unsigned *settled_all = nullptr; /* per-query settled filters (phase engine) */
   std::vector<size_t> dist_off;
   Engine eng;
   PhEngine peng; /* used when kn.engine is ADDS_ENGINE_PHASE */
@@ -1586,6 +1597,7 @@ static int batch_phase_engine(adds_batch *b) {
     q.edges = edges;
     q.split = split;
     q.dist = b->dist_all + b->dist_off[i];
+    q.settled = b->settled_all + b->dist_off[i] / 32; /* offsets are 32-word multiples */
     q.n = g->n;
     q.src = b->srcs[i];
     q.scale = b->scales[i];
@@ -1685,7 +1697,11 @@ extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs
     resolve(g, opts, &k, &b->shifts[i], &b->scales[i]);
     if (i == big) b->kn = k;
   }
+  /* a graph's tuned CTA count is for its plain solves; a batch sizes its
+   * groups itself unless the caller says otherwise */
+  b->kn.group_ctas = (opts && opts->group_ctas > 0) ? opts->group_ctas : 0;
   if (cudaMalloc(&b->dist_all, tot * 4) != cudaSuccess ||
+      cudaMalloc(&b->settled_all, tot / 8) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
       cudaEventCreate(&b->k0) != cudaSuccess || cudaEventCreate(&b->k1) != cudaSuccess) {
     cudaGetLastError();
@@ -1709,6 +1725,7 @@ extern "C" void adds_batch_free(adds_batch *b) {
   engine_free(b->eng);
   ph_engine_free(b->peng);
   if (b->dist_all) cudaFree(b->dist_all);
+  if (b->settled_all) cudaFree(b->settled_all);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->k0) cudaEventDestroy(b->k0);
@@ -2039,6 +2056,9 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
     try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
     try_field(&adds_opts::light_heavy, {0, 1, 2});
     try_field(&adds_opts::adapt, {0, 1});
+    try_field(&adds_opts::dense_scan, {-1, 4, 8});
+    /* fewer CTAs for graphs whose phases are too short to use the GPU */
+    if (g->m < (1ull << 24)) try_field(&adds_opts::group_ctas, {16, 32, 64, 148});
     if (cur.delta_shift != s0) {
       std::vector<int> s2;
       for (int d = -1; d <= 1; ++d)

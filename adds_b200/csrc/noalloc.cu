@@ -56,7 +56,9 @@ constexpr size_t kOffPt = kOffSum + 256;
 constexpr size_t kPtBytes = ((size_t)PH_NLIST << kPtnLog2) * 8;
 constexpr size_t kOffHub = (kOffPt + kPtBytes + 255) & ~size_t(255);
 constexpr size_t kOffHubSeq = kOffHub + (size_t)kHubCap * sizeof(PhHub);
-constexpr size_t kOffPool = (kOffHubSeq + (size_t)kHubCap * 4 + 4095) & ~size_t(4095);
+constexpr size_t kOffSettled = (kOffHubSeq + (size_t)kHubCap * 4 + 255) & ~size_t(255);
+constexpr size_t kSettledBytes = (size_t)ADDS_NOALLOC_MAX_N / 8; /* one bit per vertex */
+constexpr size_t kOffPool = (kOffSettled + kSettledBytes + 4095) & ~size_t(4095);
 constexpr size_t kEnd = kOffPool + (size_t)kPages * PH_PAGE * 8;
 static_assert(sizeof(PhGlobal) <= kOffGrp, "control block does not fit");
 static_assert(sizeof(PhGroup) <= kOffQd - kOffGrp, "group state does not fit");
@@ -204,6 +206,7 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   unsigned long long *pt = (unsigned long long *)(B + kOffPt);
   PhHub *hub = (PhHub *)(B + kOffHub);
   unsigned *hub_seq = (unsigned *)(B + kOffHubSeq);
+  unsigned *settled = (unsigned *)(B + kOffSettled); /* cleared by the solve's INIT phase */
   unsigned long long *pool = (unsigned long long *)(B + kOffPool);
 
   /* clear the state that must start at zero (the array keeps the previous
@@ -226,6 +229,7 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   desc.edges = (const uint2 *)edges;
   desc.split = nullptr; /* the weight-sorted copy would need memory */
   desc.dist = dist;
+  desc.settled = settled;
   desc.n = n;
   desc.src = src;
   desc.m = m;
@@ -253,6 +257,7 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   P.solo_max = 1024;
   P.adapt = 0u;
   P.lh_adapt = 1u;
+  P.dense_shift = 6u;
   P.is_float = flt ? 1u : 0u;
   P.single_src = 0xFFFFFFFFu;
   P.timeout_ns = 20000ull * 1000000ull;

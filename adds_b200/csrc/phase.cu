@@ -67,6 +67,18 @@ __device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
 __device__ __forceinline__ void red_min(unsigned *p, unsigned v) {
   asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void red_or(unsigned *p, unsigned v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+/* settled-filter word, cached in L1: the hub vertices most edges point at
+ * share a few words.  L1 is not coherent with other SMs' red.or, so a word
+ * may read a bit as still clear; that only costs the gather the bit would
+ * have saved (bits are never cleared within a launch's query). */
+__device__ __forceinline__ unsigned ld_ca32(const unsigned *p) {
+  unsigned v;
+  asm("ld.global.ca.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
 /* Edge stream load: read-only path, no L1 allocation.  An L2 evict_first
  * hint on these loads measured 2.6 % slower on R-MAT 24 (5.85 vs 5.70 ms):
  * a row's edges are often read again by the next light/heavy phase. */
@@ -304,11 +316,29 @@ __device__ void flush(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   if (tid < PH_NLIST) {
     const unsigned h = S.hist[tid];
     if (h != 0u) {
-      unsigned long long b;
-      unsigned pg[PH_RES_PAGES];
-      list_reserve(P, c, tid, h, &b, pg, &S.ptc_vp[tid], &S.ptc_pi[tid]);
-      S.bbase[tid] = b;
-      for (unsigned j = 0; j < PH_RES_PAGES; ++j) S.bpg[tid][j] = pg[j];
+      /* a dense bucket slot only records that it is non-empty (its bit);
+       * the far slot (everything past the ring) never turns dense */
+      PhGroup *G = grp_of(P, c);
+      const bool far = tid == ((S.D.base + PH_NSLOT - 1u) & (PH_NSLOT - 1u));
+      if (P.dense_shift != 0u && far && !((ld_rlx64(&G->fmask) >> tid) & 1ull))
+        atomicOr(&G->fmask, 1ull << tid);
+      const bool slot = P.dense_shift != 0u && tid < PH_NSLOT && !far &&
+                        !((ld_rlx64(&G->fmask) >> tid) & 1ull);
+      if (slot && ((ld_rlx64(&G->dmask) >> tid) & 1ull)) {
+        S.bbase[tid] = 0ull;
+        for (unsigned j = 0; j < PH_RES_PAGES; ++j) S.bpg[tid][j] = 0xFFFFFFFFu; /* no stores */
+      } else {
+        unsigned long long b;
+        unsigned pg[PH_RES_PAGES];
+        list_reserve(P, c, tid, h, &b, pg, &S.ptc_vp[tid], &S.ptc_pi[tid]);
+        S.bbase[tid] = b;
+        for (unsigned j = 0; j < PH_RES_PAGES; ++j) S.bpg[tid][j] = pg[j];
+        if (slot) {
+          const unsigned n = P.qs[S.D.q].n;
+          const unsigned long long thr = max(4096u, n >> P.dense_shift);
+          if (b + h - ld_rlx64(&G->head[tid]) > thr) atomicOr(&G->dmask, 1ull << tid);
+        }
+      }
     }
   }
   __syncthreads();
@@ -390,6 +420,9 @@ __device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOC
     ++nrepush;
     return;
   }
+  /* v's distance is at or below the bucket being settled: mark it for the
+   * settled filter (a heavy entry was marked when its light phase ran) */
+  if (mode == PH_M_LIGHT && Q.settled) red_or(Q.settled + (v >> 5), 1u << (v & 31u));
   const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
   const unsigned nl = (Q.split && !S.D.full) ? __ldg(Q.split + v) : (r1 - r0);
   if (mode == PH_M_LIGHT) {
@@ -719,19 +752,35 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   const unsigned mine = warp * 32u * U + lane; /* offset of the thread's first edge */
   if (nit) load_round(mine);
   unsigned nedges = 0;
+  const unsigned *settled = Q.settled;
   for (unsigned it = 0; it < nit; ++it) {
-    unsigned dst[U], nd[U], cur[U];
+    unsigned dst[U], nd[U], cur[U], bk[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       dst[u] = ne[u].x;
       nd[u] = 0xFFFFFFFFu;
+      bk[u] = 0u;
       if (nu[u] != 0xFFFFFFFFu) {
         nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(nu[u]), __uint_as_float(ne[u].y)))
                     : nu[u] + ne[u].y;
+        bk[u] = bucket_of<FLT>(nd[u], scale, shift);
         ++nedges;
       }
     }
     if (it + 1u < nit) load_round((it + 1u) * R + mine);
+    /* settled filter: a new distance in a later bucket than the one being
+     * settled cannot improve a vertex whose bit is set (its distance is in
+     * that bucket or below, and buckets order distances), so neither the
+     * gather nor the relaxation happens */
+    if (settled) {
+      unsigned sw[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        sw[u] = (nd[u] != 0xFFFFFFFFu && bk[u] > base) ? ld_ca32(settled + (dst[u] >> 5)) : 0u;
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if ((sw[u] >> (dst[u] & 31u)) & 1u) nd[u] = 0xFFFFFFFFu;
+    }
 #pragma unroll
     for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
     /* an improvement on the gathered value is applied with a reduction (no
@@ -743,8 +792,7 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
     for (int u = 0; u < U; ++u) {
       if (nd[u] < cur[u]) {
         red_min(dist + dst[u], nd[u]);
-        stage<BLOCK, UU>(S, dst[u], nd[u],
-                         route(bucket_of<FLT>(nd[u], scale, shift), base, P.near_far));
+        stage<BLOCK, UU>(S, dst[u], nd[u], route(bk[u], base, P.near_far));
       }
     }
     if ((it % PSmem<BLOCK, UU>::SEGI) == PSmem<BLOCK, UU>::SEGI - 1u || it + 1u == nit) {
@@ -781,6 +829,42 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
     } else {
       for (unsigned i = rank * BLOCK + tid; i < Q.n; i += gsize * BLOCK) __stcg(Q.dist + i, inf);
     }
+    if (Q.settled) {
+      const unsigned nw = (Q.n + 31u) >> 5;
+      for (unsigned i = rank * BLOCK + tid; i < nw; i += gsize * BLOCK) __stcg(Q.settled + i, 0u);
+    }
+    return;
+  }
+  if (mode == PH_M_SCAN) {
+    /* a dense bucket: every vertex whose distance lies in it goes to NEXT,
+     * once, with its current distance.  Tiles of 4 x BLOCK vertices are
+     * dealt round-robin over the group's CTAs (one 16-byte load per thread);
+     * nothing relaxes in this phase, so the distances do not move. */
+    const unsigned base = S.D.base, n = Q.n;
+    const unsigned inf = P.is_float ? 0x7F7FFFFFu : 0x7FFFFFFFu;
+    const bool vec = (reinterpret_cast<unsigned long long>(Q.dist) & 15ull) == 0ull;
+    const unsigned ntile = (n + 4u * BLOCK - 1u) / (4u * BLOCK);
+    for (unsigned t = solo ? 0u : c.rank; t < ntile; t += solo ? 1u : P.gsize) {
+      const unsigned v0 = t * 4u * BLOCK + 4u * tid;
+      unsigned d[4];
+      if (vec && v0 + 3u < n) {
+        const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(Q.dist + v0));
+        d[0] = x.x;
+        d[1] = x.y;
+        d[2] = x.z;
+        d[3] = x.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[j] = (v0 + j < n) ? __ldcg(Q.dist + v0 + j) : inf;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (d[j] != inf && bucket_of<FLT>(d[j], Q.scale, Q.shift) == base)
+          stage<BLOCK, UU>(S, v0 + j, d[j], PH_LNEXT);
+      __syncthreads();
+      if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+    }
+    flush<BLOCK, UU>(P, c, S);
     return;
   }
   const unsigned base = S.D.base;
@@ -871,7 +955,10 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       /* the source's bucket counts as dense: it starts with split rows */
       st_rlx32(&G->lh_dense, 1u);
       st_rlx32(&G->lh_k, 0u);
+      st_rlx32(&G->lh_full, 0u);
       st_rlx64(&G->lh_prev, 0ull);
+      st_rlx64(&G->dmask, 0ull);
+      st_rlx64(&G->fmask, 0ull);
       __threadfence();
     }
     __syncwarp();
@@ -902,11 +989,13 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         /* another light phase of the same bucket: when it re-improved few of
          * the vertices the last one expanded (under 1 in 20), heavy edges go
          * with the light ones, and a bucket whose second light phase is that
-         * small marks the next bucket as sparse */
+         * small marks the next bucket as sparse.  The first light phase of a
+         * bucket collected by a scan (or of the source's bucket) takes the
+         * choice made when the bucket opened. */
         const unsigned long long prevc = ld_rlx64(&G->lh_prev);
         const bool few = (tn - hn) * 20ull < prevc;
         const unsigned k = ld_rlx32(&G->lh_k);
-        full = few ? 1u : 0u;
+        full = k == 0u ? ld_rlx32(&G->lh_full) : (few ? 1u : 0u);
         if (lane == 0) {
           if (k == 1u && !few) st_rlx32(&G->lh_dense, 1u);
           st_rlx64(&G->lh_prev, tn - hn);
@@ -957,9 +1046,30 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         tb = ld_rlx64(&G->tails[sb].tail);
         hb = ld_rlx64(&G->head[sb]);
       }
-      const unsigned ma = __ballot_sync(0xFFFFFFFFu, ta > ha);
-      const unsigned mb = __ballot_sync(0xFFFFFFFFu, offb < PH_NSLOT && tb > hb);
-      if (ma | mb) {
+      /* a dense slot is non-empty whatever its list holds */
+      const unsigned long long dm = P.dense_shift ? ld_rlx64(&G->dmask) : 0ull;
+      const unsigned ma = __ballot_sync(0xFFFFFFFFu, ta > ha || ((dm >> sa) & 1ull));
+      const unsigned mb =
+          __ballot_sync(0xFFFFFFFFu, offb < PH_NSLOT && (tb > hb || ((dm >> sb) & 1ull)));
+      const unsigned long long m0 = (unsigned long long)ma | ((unsigned long long)mb << 32);
+      const unsigned s0 = m0 ? (base + (unsigned)__ffsll((long long)m0)) & (PH_NSLOT - 1u) : 0u;
+      if (m0 != 0ull && ((dm >> s0) & 1ull)) {
+        /* the nearest bucket is dense: collect it with one pass over the
+         * distances (its list is incomplete and is dropped) */
+        mode = PH_M_SCAN;
+        list = s0;
+        base += (unsigned)__ffsll((long long)m0);
+        lo = 0ull;
+        hi = P.qs[q].n;
+        if (lane == 0) {
+          st_rlx32(&G->base, base);
+          st_rlx64(&G->head[s0], ld_rlx64(&G->tails[s0].tail));
+          atomicAnd(&G->dmask, ~(1ull << s0));
+          st_rlx32(&G->lh_full, ld_rlx32(&G->lh_dense) != 0u ? 0u : 1u);
+          st_rlx32(&G->lh_dense, 0u);
+          st_rlx32(&G->lh_k, 0u);
+        }
+      } else if (ma | mb) {
         /* the nearest non-empty slot; with adaptation on, while the entries
          * gathered stay few, the next non-empty slots too (at most PH_MAXR,
          * never the far slot after another): the bucket is widened on the
@@ -978,6 +1088,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
           const unsigned long long t = __shfl_sync(0xFFFFFFFFu, i < 32u ? ta : tb, i & 31u);
           const unsigned long long h = __shfl_sync(0xFFFFFFFFu, i < 32u ? ha : hb, i & 31u);
           const unsigned sl = (base + off) & (PH_NSLOT - 1u);
+          if (top != 0u && ((dm >> sl) & 1ull)) break; /* a dense slot opens alone */
           if (top == 0u) {
             list = sl;
             lo = h;
@@ -1012,6 +1123,11 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     if ((mode == PH_M_LIGHT || mode == PH_M_HEAVY) && lane == 0) {
       st_rlx64(&G->head[list], hi);
       for (unsigned r = 0; r < nx; ++r) st_rlx64(&G->head[xl[r]], xhi[r]);
+      if (P.dense_shift) { /* opened slots: their far entries move on now */
+        unsigned long long opened = list < PH_NSLOT ? (1ull << list) : 0ull;
+        for (unsigned r = 0; r < nx; ++r) opened |= 1ull << xl[r];
+        if (opened) atomicAnd(&G->fmask, ~opened);
+      }
       st_rlx32(&G->hub_count, 0u); /* split rows of the coming phase */
       st_rlx32(&G->hub_claim, 0u);
     }
@@ -1451,8 +1567,11 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
     return -5;
   const int cps = (k.ctas_per_sm > 0 && k.ctas_per_sm < bps) ? k.ctas_per_sm : bps;
   const unsigned nctas = (unsigned)(cps * E.num_sms);
+  E.req_group = k.group_ctas;
   if (E.nq == 1) {
-    E.gsize = nctas;
+    /* one query: every resident CTA, or fewer when asked (a small graph's
+     * phases are short, and a group barrier over fewer CTAs is cheaper) */
+    E.gsize = k.group_ctas > 0 ? std::min((unsigned)k.group_ctas, nctas) : nctas;
     E.groups = 1;
   } else {
     /* about 32 groups: enough to run small queries side by side, large
@@ -1549,6 +1668,7 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->adapt = k.adapt;
   P->lh_adapt = k.lh_adapt;
   P->near_far = k.near_far ? 1u : 0u;
+  P->dense_shift = k.near_far ? 0u : k.dense_shift;
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

@@ -38,6 +38,7 @@
 #define PH_M_HEAVY 2u  /* expand heavy edges of settled vertices              */
 #define PH_M_HUB 3u    /* (reserved: split rows are expanded inside their phase) */
 #define PH_M_EXIT 4u   /* no more queries for this group                      */
+#define PH_M_SCAN 6u   /* collect a dense bucket from the distances into NEXT  */
 
 /* device error codes (first one wins) */
 #define PH_ERR_TIMEOUT 1u
@@ -54,6 +55,12 @@ struct PhQuery {
                             split != NULL                                     */
   const unsigned *split; /* light edges (w < delta) at the start of each row  */
   unsigned *dist;        /* n distance words                                  */
+  /* settled filter, ceil(n/32) words or NULL: bit v set => bucket(dist[v])
+   * is at or below the bucket being settled (set when v is expanded from its
+   * bucket; both only move one way within a solve).  A relaxation whose new
+   * distance lands above the current bucket cannot improve such a vertex,
+   * so it is skipped without gathering dist[v]. */
+  unsigned *settled;
   unsigned n;
   unsigned src;
   float scale;           /* float graphs: key = floor(d * scale)              */
@@ -125,7 +132,18 @@ struct __align__(128) PhGroup {
   /* near-far schedule: smallest bucket pushed to the far list since the
    * threshold last moved */
   unsigned far_min;
-  unsigned pad5[15];
+  /* first light phase of a bucket opened by a scan: whole rows or not */
+  unsigned lh_full;
+  unsigned pad5[14];
+  /* dense bucket slots (bit per slot): a slot whose pushes passed the dense
+   * threshold stops storing entries; its bucket is collected by a scan of
+   * the distances when it opens (PH_M_SCAN) */
+  unsigned long long dmask;
+  /* slots holding far-slot entries (buckets beyond the ring when they were
+   * pushed): such a slot never turns dense, since a scan collects one bucket
+   * only; the bit clears when the slot opens and its entries move on */
+  unsigned long long fmask;
+  unsigned long long pad6[14];
   unsigned long long head[PH_NLIST];
   PhTail tails[PH_NLIST];
 };
@@ -182,6 +200,9 @@ struct PhParams {
   unsigned adapt;              /* merge thin bucket slots into one phase      */
   unsigned lh_adapt;           /* whole rows in light phases of sparse buckets */
   unsigned near_far;           /* two lists instead of the bucket ring         */
+  unsigned dense_shift;        /* a bucket slot that receives more than
+                                  max(n >> dense_shift, 4096) pushes turns
+                                  dense (collected by a scan); 0 = never      */
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
@@ -198,6 +219,7 @@ struct PhEngine {
   int device = -1;
   bool flt = false;
   unsigned nq = 0, groups = 0, gsize = 0, block = 0, variant = 0;
+  int req_group = 0; /* group_ctas knob the engine was sized with */
   unsigned pages_per_group = 0, ptn_log2 = 0, hub_cap = 0, max_n = 0;
   unsigned hub_eff = 0; /* split-row chunk length the record store is sized for */
   PhGroup *grp = nullptr;
@@ -222,6 +244,7 @@ struct PhKnobs {
   int group_ctas;     /* CTAs per group (batches); <= 0: automatic            */
   unsigned hub_threshold, hub_chunk, solo_max, adapt, lh_adapt;
   unsigned near_far;  /* near-far schedule instead of the bucket ring          */
+  unsigned dense_shift; /* dense bucket slots (PhParams::dense_shift), 0 = off  */
   unsigned long long timeout_ns;
 };
 

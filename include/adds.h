@@ -85,8 +85,10 @@ typedef struct adds_opts {
   int32_t greed;         /* async engine: a claim takes avail / (CTAs >> greed)
                             entries; <0 = auto                                 */
   int32_t engine;        /* ADDS_ENGINE_*: 0 = auto (phase)                      */
-  int32_t group_ctas;    /* phase engine, batches: CTAs that solve one query
-                            together; 0 = auto                                 */
+  int32_t group_ctas;    /* phase engine: CTAs that solve one query together
+                            (batches: the group size; plain solves: the CTAs
+                            launched, fewer making each phase's barrier
+                            cheaper on small graphs); 0 = auto              */
   int32_t solo_max;      /* phase engine: frontiers of at most this many entries
                             run on one CTA without a group barrier; <0 = auto  */
   int32_t near_far;      /* phase engine, 1: near-far schedule (the Galois GPU
@@ -94,7 +96,12 @@ typedef struct adds_opts {
                             of the bucket ring, split against a threshold that
                             moves one bucket at a time (or to the smallest
                             bucket in the pile); 0 = bucket ring             */
-  int32_t reserved[4];
+  int32_t dense_scan;    /* phase engine: a bucket slot that receives more than
+                            max(n >> dense_scan, 4096) pushes stops storing
+                            them, and its bucket is collected by one pass over
+                            the distances when it opens (no duplicate or stale
+                            entries); 0 = auto (6), < 0 = off                */
+  int32_t reserved[3];
 } adds_opts;
 
 /* Engines.  PHASE settles the buckets in bulk-synchronous phases (light
@@ -308,7 +315,8 @@ int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_start,
 typedef struct adds_phase_trace {
   uint64_t t_ns;  /* device clock at the decision, ns                       */
   uint32_t count; /* frontier entries (split rows: chunks; init: vertices)   */
-  uint16_t mode;  /* 0 init, 1 light, 2 heavy, 3 split rows, 4 exit;
+  uint16_t mode;  /* 0 init, 1 light, 2 heavy, 3 split rows, 4 exit,
+                     6 scan (a dense bucket collected from the distances);
                      | 0x100 when one CTA ran it alone                      */
   uint16_t base;  /* low 16 bits of the bucket being settled                */
   uint32_t edges;   /* edges the phase relaxed                              */

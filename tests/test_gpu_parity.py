@@ -195,6 +195,69 @@ def test_phase_trace_and_stats():
     assert st["engine"] == PHASE and st["ctas"] > 0
 
 
+@pytest.mark.parametrize("dense", [-1, 6, 20])
+@pytest.mark.parametrize("lh", [0, 1, 2])
+@pytest.mark.parametrize("adapt", [0, 1])
+def test_dense_bucket_scan(dense, lh, adapt):
+    """Dense bucket slots (dense_scan > 0): a slot that received more than
+    max(n >> dense_scan, 4096) pushes stops storing them and its bucket is
+    collected by a scan of the distances when it opens.  Distances stay the
+    oracle's (int R-MAT, float grid); with the scan on, the trace shows scan
+    phases (mode 6) on the R-MAT, whose big buckets pass the threshold."""
+    g = G.rmat(15, 16, seed=24, w_hi=10000)
+    src = G.max_degree_vertex(g)
+    dg = A.Graph.from_csr(g)
+    try:
+        dg.trace(1 << 16)
+        d, st = dg.sssp(src, A.default_opts(**OPTS, engine=PHASE, delta_shift=8, light_heavy=lh,
+                                            adapt=adapt, dense_scan=dense))
+        tr, n = dg.trace_read(1 << 16)
+        dg.trace(0)
+    finally:
+        dg.close()
+    ref, _ = O.dijkstra(g, src)
+    assert np.array_equal(d, ref)
+    scans = int(((tr["mode"] & 0xFF) == 6).sum())
+    if dense < 0:
+        assert scans == 0
+    else:
+        assert scans > 0
+    f = G.grid(128, 96, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=25)
+    _check(f, 48 * 128 + 64, engine=PHASE, delta_shift=14, light_heavy=lh, adapt=adapt,
+           dense_scan=dense)
+
+
+@pytest.mark.parametrize("ctas", [1, 16, 64])
+def test_plain_solve_with_few_ctas(ctas):
+    """group_ctas on a plain solve launches that many CTAs (a cheaper group
+    barrier for small graphs); the distances stay the oracle's."""
+    g = G.rmat(14, 16, seed=26, w_hi=1000)
+    st = _check(g, G.max_degree_vertex(g), engine=PHASE, group_ctas=ctas)
+    assert st["ctas"] == ctas
+    f = G.grid(64, 48, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=27)
+    _check(f, 24 * 64 + 32, engine=PHASE, group_ctas=ctas)
+
+
+def test_dense_bucket_scan_batch():
+    """Dense slots per query inside one batched launch (each query's scan
+    reads its own distances)."""
+    gs = [G.rmat(13, 16, seed=30 + i, w_hi=10000) for i in range(3)]
+    dgs = [A.Graph.from_csr(g) for g in gs]
+    try:
+        srcs = [G.max_degree_vertex(g) for g in gs]
+        b = A.Batch(dgs + dgs, srcs + [1, 2, 3],
+                    A.default_opts(engine=PHASE, delta_shift=7, dense_scan=20, **OPTS))
+        for _ in range(2):
+            b.run()
+            for q, (g, s) in enumerate(zip(gs + gs, srcs + [1, 2, 3])):
+                ref, _ = O.dijkstra(g, s)
+                assert np.array_equal(b.dist(q), ref), q
+        b.close()
+    finally:
+        for x in dgs:
+            x.close()
+
+
 @pytest.mark.parametrize("variant", VARIANTS[:3])
 @pytest.mark.parametrize("lh", [0, 1, 2])
 def test_phase_schedules_float_grid(variant, lh):
