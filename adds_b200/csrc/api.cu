@@ -267,7 +267,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
-  int engine, variant, group_ctas, solo_max, near_far, dense_scan; /* phase engine */
+  int engine, variant, group_ctas, solo_max, near_far, dense_scan, tma_rows; /* phase engine */
   unsigned long long timeout_ns;
 };
 
@@ -292,6 +292,7 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.lh_adapt = k.light_heavy == 2 ? 1u : 0u;
   p.near_far = k.near_far ? 1u : 0u;
   p.dense_shift = (k.dense_scan > 0 && !k.near_far) ? (unsigned)std::min(k.dense_scan, 31) : 0u;
+  p.tma_rows = k.tma_rows > 0 ? 1u : 0u;
   p.timeout_ns = k.timeout_ns;
   return p;
 }
@@ -1027,6 +1028,7 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   /* dense bucket slots: explicit > tuned > 6 (a slot holding more than n/64
    * pushes is cheaper to collect with one pass over the distances) */
   k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : 6);
+  k->tma_rows = o->tma_rows > 0 ? 1 : (t->tma_rows > 0 ? 1 : 0);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -1186,6 +1188,7 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.m = g->m;
   PhEngine &E = g->peng;
   if (E.nq == 1 && E.variant == (unsigned)k.variant && E.req_group == k.group_ctas &&
+      E.tma == (k.tma_rows > 0 ? 1u : 0u) &&
       ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
     PhQuery &h = E.qs_host[0];
     if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)

@@ -171,9 +171,16 @@ __device__ bool slot_reserve(const EngParams &P, const QueryDesc &d, unsigned s,
   const unsigned long long base = atomicAdd(&sc->tail, (unsigned long long)c);
   *pbase = base;
   *pp0 = *pp1 = PI_BAD;
+  /* span of live entries the page-table ring must cover.  head is read after
+   * the reservation: other CTAs may meanwhile have published later ranges
+   * and claimers may have moved head past this (still unwritten) range,
+   * whose entries they then wait for.  head > base + c is therefore legal
+   * and means a short span; the unsigned difference must not wrap into a
+   * spurious overflow. */
   const unsigned long long head = ld_rlx64(&sc->head);
   const unsigned long long ptn = 1ull << d.ptn_log2;
-  if (base + c - head > (ptn - 3ull) * ADDS_PAGE) {
+  const unsigned long long end = base + c;
+  if (end > head && end - head > (ptn - 3ull) * ADDS_PAGE) {
     raise_err(P.g, ADDS_DEV_OVERFLOW, W_SPAN);
     return false;
   }

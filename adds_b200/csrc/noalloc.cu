@@ -189,8 +189,8 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
     void *p = nullptr;
     NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     int bps_i = 0, bps_f = 0, sms = 0;
-    NA_CK(adds_phase_prepare(false, kVariant, &bps_i));
-    NA_CK(adds_phase_prepare(true, kVariant, &bps_f));
+    NA_CK(adds_phase_prepare(false, kVariant, false, &bps_i));
+    NA_CK(adds_phase_prepare(true, kVariant, false, &bps_f));
     NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bps = bps_i < bps_f ? bps_i : bps_f;
     if (bps < 1) return ADDS_ERR_UNSUPPORTED;

@@ -88,6 +88,48 @@ __device__ __forceinline__ uint2 ld_edge(const uint2 *p) {
   return r;
 }
 
+/* bulk-copy staging (PTX ISA: mbarrier, cp.async.bulk).  One mbarrier per
+ * CTA counts one arrival (thread 0) plus the bytes of every copy; the
+ * copies go to this CTA's own shared memory, never with multicast. */
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+/* 1-D bulk copy global -> this CTA's shared memory; both addresses and the
+ * size are multiples of 16 bytes */
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+/* generic-proxy accesses of shared memory before async-proxy writes to it */
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 enum : unsigned { W_BARRIER = 1, W_PT = 2, W_ALLOC = 3, W_MAPPING = 4, W_HUB = 5, W_COPY = 6 };
 
 __device__ __forceinline__ void raise_err(PhGlobal *g, unsigned code, unsigned where) {
@@ -173,7 +215,19 @@ struct PSmem {
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
   unsigned hub_made; /* this CTA cut a row into records in the current phase */
   unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
+  /* bulk-copy staging of split-row chunks (tma_rows): the mbarrier, its
+   * phase parity, and whether the chunk's edges are in shared memory */
+  unsigned long long tma_bar;
+  unsigned tma_par, ck_tma;
 };
+
+/* the staging area of the bulk copies: PH_TMA_BYTES of dynamic shared
+ * memory past PSmem (present only in launches with tma_rows) */
+template <int BLOCK, int UU>
+__device__ __forceinline__ uint2 *tma_buf(PSmem<BLOCK, UU> &S) {
+  return reinterpret_cast<uint2 *>(reinterpret_cast<unsigned char *>(&S) +
+                                   ((sizeof(PSmem<BLOCK, UU>) + 15u) & ~(size_t)15u));
+}
 
 /* what a CTA keeps for the kernel's lifetime; the group's arrays are
  * recomputed from the parameters where they are used */
@@ -493,6 +547,7 @@ __device__ __forceinline__ void finish_items(PSmem<BLOCK, UU> &S, unsigned k, un
     S.it_off[EPT * BLOCK] = tot;
     S.ck_k = k;
     S.ck_E = tot;
+    S.ck_tma = 0u; /* frontier chunks read the edge array directly */
   }
   __syncthreads();
 }
@@ -623,7 +678,10 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
  * false when no record is left.  Every thread calls it. */
 template <bool FLT, int BLOCK, int UU>
 __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
-  constexpr unsigned K = PH_HUB_PER_CLAIM(BLOCK);
+  /* with bulk-copy staging a claim takes as many records as the staging
+   * area holds */
+  const unsigned K = P.tma_rows ? min(PH_TMA_REC, PH_HUB_PER_CLAIM(BLOCK))
+                                : PH_HUB_PER_CLAIM(BLOCK);
   const unsigned tid = threadIdx.x;
   PhGroup *G = grp_of(P, c);
   const PhQuery &Q = P.qs[S.D.q];
@@ -675,6 +733,18 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
         rb = h.z;
         re = h.w;
         du = h.y;
+        if (P.tma_rows) {
+          /* stage the chunk in this CTA's shared memory: edge indices
+           * widened to even (16-byte boundaries; the edge array is padded
+           * past m); the item then indexes the staging slot */
+          const unsigned e0 = h.z & ~1u, e1 = (h.w + 1u) & ~1u;
+          uint2 *slot = tma_buf(S) + tid * PH_TMA_EDGES;
+          fence_proxy_async_smem();
+          mbar_expect_tx(&S.tma_bar, (e1 - e0) * 8u);
+          bulk_g2s(slot, Q.edges + e0, (e1 - e0) * 8u, &S.tma_bar);
+          rb = tid * PH_TMA_EDGES + (h.z - e0);
+          re = rb + (h.w - h.z);
+        }
       } else {
         stale = true;
       }
@@ -683,6 +753,32 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
   S.it_rb[tid] = rb;
   S.it_du[tid] = du;
   const unsigned nstale = __syncthreads_count(stale);
+  if (P.tma_rows) {
+    /* every expected byte count is registered: one arrival completes the
+     * phase once the copies have landed.  The wait is bounded; on a
+     * timeout the error word is set and the chunk is dropped (the solve
+     * ends with the error) */
+    if (tid == 0) mbar_arrive(&S.tma_bar);
+    const unsigned par = S.tma_par;
+    bool done = false;
+    for (unsigned it = 0; it < (1u << 22); ++it) {
+      if (mbar_try_wait(&S.tma_bar, par)) {
+        done = true;
+        break;
+      }
+      if ((it & 1023u) == 1023u && gtimer() > c.deadline) break;
+    }
+    if (!done) {
+      raise_err(P.g, PH_ERR_TIMEOUT, W_COPY);
+      rb = re = 0u;
+      S.it_rb[tid] = 0u;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      S.tma_par = par ^ 1u;
+      S.ck_tma = 1u;
+    }
+  }
   if (tid == 0) {
     S.st_stale += nstale;
     S.st_hubs += k - nstale;
@@ -694,6 +790,7 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
     S.it_off[BLOCK] = tot;
     S.ck_k = k;
     S.ck_E = tot;
+    S.ck_tma = P.tma_rows ? 1u : 0u;
   }
   __syncthreads();
   return true;
@@ -720,6 +817,8 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   const float scale = Q.scale;
   const unsigned shift = Q.shift;
   const unsigned *off = S.it_off; /* off[k] = E */
+  const bool staged = S.ck_tma != 0u; /* split-row chunk edges in shared memory */
+  const uint2 *tb = tma_buf(S);
   unsigned lo = 0; /* item of the thread's last edge: its edges only move forward */
   uint2 ne[U];
   unsigned nu[U];
@@ -744,7 +843,8 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
       ne[u] = make_uint2(0u, 0u);
       if (e < E) {
         find(e);
-        ne[u] = ld_edge(edges + S.it_rb[lo] + (e - off[lo]));
+        ne[u] = staged ? tb[S.it_rb[lo] + (e - off[lo])]
+                       : ld_edge(edges + S.it_rb[lo] + (e - off[lo]));
         nu[u] = S.it_du[lo];
       }
     }
@@ -1282,6 +1382,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     S.st_hubs = S.st_solo = 0;
     S.tr_e = S.tr_mi = S.tr_mp = 0ull;
     for (int i = 0; i < 8; ++i) S.cy[i] = 0ull;
+    S.ck_tma = 0u;
+    S.tma_par = 0u;
+    if (P.tma_rows) {
+      mbar_init(&S.tma_bar, 1u);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
   }
   if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
@@ -1395,14 +1501,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   }
 }
 
+/* dynamic shared memory of a launch: PSmem, plus the bulk-copy staging
+ * area when split-row chunks are staged (tma_rows) */
+template <int BLOCK, int MINB>
+static size_t smem_bytes(bool tma) {
+  const size_t s = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
+  return tma ? ((s + 15u) & ~(size_t)15u) + PH_TMA_BYTES : s;
+}
+
 template <bool FLT, int BLOCK, int MINB>
-static cudaError_t prep_one(int *max_blocks_per_sm) {
-  const size_t smem = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
+static cudaError_t prep_one(bool tma, int *max_blocks_per_sm) {
   cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_bytes<BLOCK, MINB>(true));
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
-                                                       phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      max_blocks_per_sm, phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem_bytes<BLOCK, MINB>(tma));
 }
 
 template <bool FLT, int BLOCK, int MINB>
@@ -1412,7 +1526,7 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P.groups * P.gsize);
   cfg.blockDim = dim3(BLOCK);
-  cfg.dynamicSmemBytes = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
+  cfg.dynamicSmemBytes = smem_bytes<BLOCK, MINB>(P.tma_rows != 0u);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -1486,10 +1600,11 @@ int adds_phase_variant_block(int variant) {
   return 0;
 }
 
-cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm) {
+cudaError_t adds_phase_prepare(bool flt, int variant, bool tma, int *max_blocks_per_sm) {
   using namespace adds_phase;
 #define X(i, b, m) \
-  if (variant == i) return flt ? prep_one<true, b, m>(max_blocks_per_sm) : prep_one<false, b, m>(max_blocks_per_sm);
+  if (variant == i) \
+    return flt ? prep_one<true, b, m>(tma, max_blocks_per_sm) : prep_one<false, b, m>(tma, max_blocks_per_sm);
   PH_VARIANTS(X)
 #undef X
   return cudaErrorInvalidValue;
@@ -1547,8 +1662,8 @@ int ph_engine_upload(PhEngine &E, cudaStream_t st) {
   return 0;
 }
 
-static int ph_blocks_per_sm(bool flt, int variant, int *bps) {
-  return adds_phase_prepare(flt, variant, bps) == cudaSuccess ? 0 : -5;
+static int ph_blocks_per_sm(bool flt, int variant, bool tma, int *bps) {
+  return adds_phase_prepare(flt, variant, tma, bps) == cudaSuccess ? 0 : -5;
 }
 
 /* Sizes the per-group pools for the largest query (x grow) and allocates. */
@@ -1561,7 +1676,8 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
   E.variant = (unsigned)k.variant;
   E.block = (unsigned)adds_phase_variant_block(k.variant);
   int bps = 0;
-  if (E.block == 0 || ph_blocks_per_sm(flt, k.variant, &bps) || bps < 1)
+  E.tma = k.tma_rows ? 1u : 0u;
+  if (E.block == 0 || ph_blocks_per_sm(flt, k.variant, E.tma != 0u, &bps) || bps < 1)
     return -9; /* ADDS_ERR_UNSUPPORTED */
   if (cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
     return -5;
@@ -1642,7 +1758,8 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
 
 unsigned ph_hub_chunk(const PhKnobs &k) {
   const unsigned thr = std::max(64u, k.hub_threshold);
-  return std::max(64u, std::min(k.hub_chunk, thr));
+  const unsigned c = std::max(64u, std::min(k.hub_chunk, thr));
+  return k.tma_rows ? std::min(c, PH_TMA_CHUNK) : c; /* a staging slot holds 256 edges */
 }
 
 int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P) {
@@ -1669,6 +1786,8 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->lh_adapt = k.lh_adapt;
   P->near_far = k.near_far ? 1u : 0u;
   P->dense_shift = k.near_far ? 0u : k.dense_shift;
+  P->tma_rows = (k.tma_rows && E.tma) ? 1u : 0u;
+  if (k.tma_rows && !E.tma) return -9; /* engine sized without the staging area */
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

@@ -227,6 +227,21 @@ def test_dense_bucket_scan(dense, lh, adapt):
            dense_scan=dense)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("lh", [0, 2])
+def test_split_rows_staged_by_bulk_copies(variant, lh):
+    """tma_rows 1: split-row chunks reach shared memory by cp.async.bulk
+    (mbarrier-completed) before their edges are relaxed; the distances stay
+    the oracle's (int R-MAT with many split rows, float grid)."""
+    g = G.rmat(14, 16, seed=28, w_hi=10000)
+    st = _check(g, G.max_degree_vertex(g), engine=PHASE, tma_rows=1, hub_threshold=64,
+                light_heavy=lh, block_threads=variant[0], ctas_per_sm=variant[1])
+    assert st["hub_chunks"] > 0
+    f = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=29)
+    _check(f, 40 * 96 + 48, engine=PHASE, tma_rows=1, hub_threshold=64, light_heavy=lh,
+           block_threads=variant[0], ctas_per_sm=variant[1])
+
+
 @pytest.mark.parametrize("ctas", [1, 16, 64])
 def test_plain_solve_with_few_ctas(ctas):
     """group_ctas on a plain solve launches that many CTAs (a cheaper group
