@@ -1094,6 +1094,17 @@ static int graph_sorted(adds_graph *g) {
                                                       (int)g->n, g->row, g->row + 1, g->stream);
   if (e == cudaSuccess) k_zip<<<592, 256, 0, g->stream>>>(wk2, dv2, m, g->sedges);
   if (e != cudaSuccess) return cuda_fail(e, "segmented sort");
+  if (m > (1ull << 24)) {
+    /* a large graph's sort buffers (16 B per edge, plus CUB's) are not kept:
+     * weight updates that need a re-sort are rare there, and the memory is
+     * better left to the solver */
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->sort_buf);
+    g->sort_buf = nullptr;
+    cudaFree(g->sort_tmp);
+    g->sort_tmp = nullptr;
+    g->sort_tmp_bytes = 0;
+  }
   g->sorted_valid = true;
   g->split_valid = false;
   return ADDS_OK;

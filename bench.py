@@ -114,6 +114,7 @@ WORKLOADS = {
                    src="maxdeg"),
     "rmat21": dict(kind="rmat", scale=21, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=21),
     "rmat22": dict(kind="rmat", scale=22, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=22),
+    "rmat23": dict(kind="rmat", scale=23, wtype=0, w_lo=1, w_hi=10000, nsrc=8, seed=23),
     "grid4096": dict(kind="grid", side=4096, wtype=1, w_lo=1.0, w_hi=100.0, nsrc=1, seed=4096,
                      src="center"),
 }
