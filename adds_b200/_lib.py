@@ -60,8 +60,7 @@ class Opts(C.Structure):
         ("solo_max", C.c_int32),
         ("near_far", C.c_int32),
         ("dense_scan", C.c_int32),
-        ("tma_rows", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -267,7 +267,7 @@ static int engine_alloc(Engine &E, int device, bool flt, const std::vector<EngQu
 struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
-  int engine, variant, group_ctas, solo_max, near_far, dense_scan, tma_rows; /* phase engine */
+  int engine, variant, group_ctas, solo_max, near_far, dense_scan; /* phase engine */
   unsigned long long timeout_ns;
 };
 
@@ -292,7 +292,6 @@ static PhKnobs phase_knobs(const Knobs &k) {
   p.lh_adapt = k.light_heavy == 2 ? 1u : 0u;
   p.near_far = k.near_far ? 1u : 0u;
   p.dense_shift = (k.dense_scan > 0 && !k.near_far) ? (unsigned)std::min(k.dense_scan, 31) : 0u;
-  p.tma_rows = k.tma_rows > 0 ? 1u : 0u;
   p.timeout_ns = k.timeout_ns;
   return p;
 }
@@ -390,7 +389,6 @@ struct adds_graph {
   unsigned *row = nullptr;
   uint2 *edges = nullptr;
   unsigned *dist = nullptr;
-  unsigned *settled = nullptr; /* phase engine settled filter, ceil(n/32) words */
   uint2 *sedges = nullptr;     /* rows sorted by weight (light edges first)   */
   unsigned *split = nullptr;   /* light-edge count per row for split_thr      */
   unsigned split_thr = 0;
@@ -536,8 +534,6 @@ static int graph_finish(adds_graph *g) {
   g->avg_w = ns ? sw / ns : 1.0;
   CK(cudaMalloc(&g->dist, ((size_t)g->n ? g->n : 1) * 4));
   g->bytes += (size_t)g->n * 4;
-  CK(cudaMalloc(&g->settled, (((size_t)g->n + 31) / 32) * 4));
-  g->bytes += (((size_t)g->n + 31) / 32) * 4;
   CK(cudaEventCreate(&g->ev0));
   CK(cudaEventCreate(&g->ev1));
   return ADDS_OK;
@@ -565,7 +561,6 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->row) cudaFree(g->row);
   if (g->edges) cudaFree(g->edges);
   if (g->dist) cudaFree(g->dist);
-  if (g->settled) cudaFree(g->settled);
   if (g->sedges) cudaFree(g->sedges);
   if (g->split) cudaFree(g->split);
   if (g->aux) cudaFree(g->aux);
@@ -1028,7 +1023,6 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   /* dense bucket slots: explicit > tuned > 6 (a slot holding more than n/64
    * pushes is cheaper to collect with one pass over the distances) */
   k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : 6);
-  k->tma_rows = o->tma_rows > 0 ? 1 : (t->tma_rows > 0 ? 1 : 0);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -1191,7 +1185,6 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.edges = edges;
   q.split = split;
   q.dist = g->dist;
-  q.settled = g->settled;
   q.n = g->n;
   q.src = 0;
   q.scale = scale;
@@ -1199,7 +1192,6 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.m = g->m;
   PhEngine &E = g->peng;
   if (E.nq == 1 && E.variant == (unsigned)k.variant && E.req_group == k.group_ctas &&
-      E.tma == (k.tma_rows > 0 ? 1u : 0u) &&
       ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
     PhQuery &h = E.qs_host[0];
     if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)
@@ -1580,7 +1572,6 @@ struct adds_batch {
   std::vector<adds_graph *> ugraph; /* distinct graphs, first-use order */
   std::vector<unsigned> qgid;
   unsigned *dist_all = nullptr;
-  unsigned *settled_all = nullptr; /* per-query settled filters (phase engine) */
   std::vector<size_t> dist_off;
   Engine eng;
   PhEngine peng; /* used when kn.engine is ADDS_ENGINE_PHASE */
@@ -1611,7 +1602,6 @@ static int batch_phase_engine(adds_batch *b) {
     q.edges = edges;
     q.split = split;
     q.dist = b->dist_all + b->dist_off[i];
-    q.settled = b->settled_all + b->dist_off[i] / 32; /* offsets are 32-word multiples */
     q.n = g->n;
     q.src = b->srcs[i];
     q.scale = b->scales[i];
@@ -1715,7 +1705,6 @@ extern "C" int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs
    * groups itself unless the caller says otherwise */
   b->kn.group_ctas = (opts && opts->group_ctas > 0) ? opts->group_ctas : 0;
   if (cudaMalloc(&b->dist_all, tot * 4) != cudaSuccess ||
-      cudaMalloc(&b->settled_all, tot / 8) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
       cudaEventCreate(&b->k0) != cudaSuccess || cudaEventCreate(&b->k1) != cudaSuccess) {
     cudaGetLastError();
@@ -1739,7 +1728,6 @@ extern "C" void adds_batch_free(adds_batch *b) {
   engine_free(b->eng);
   ph_engine_free(b->peng);
   if (b->dist_all) cudaFree(b->dist_all);
-  if (b->settled_all) cudaFree(b->settled_all);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->k0) cudaEventDestroy(b->k0);
@@ -2033,6 +2021,19 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
     if (ma < bm) {
       bm = ma;
       cur = alt;
+    }
+    /* small graphs: the phase engine on fewer CTAs (cheaper barriers) is a
+     * candidate of its own before the engine is chosen */
+    if (g->m < (1ull << 24)) {
+      for (int gc : {16, 32, 64}) {
+        adds_opts t = defaults(ADDS_ENGINE_PHASE);
+        t.group_ctas = gc;
+        const double ms = time_solves(g, srcs, ns, &t);
+        if (ms < bm) {
+          bm = ms;
+          cur = t;
+        }
+      }
     }
   }
   resolve(g, &cur, &k, &s0, &sc); /* knobs of the chosen engine */

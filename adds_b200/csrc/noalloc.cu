@@ -56,9 +56,7 @@ constexpr size_t kOffPt = kOffSum + 256;
 constexpr size_t kPtBytes = ((size_t)PH_NLIST << kPtnLog2) * 8;
 constexpr size_t kOffHub = (kOffPt + kPtBytes + 255) & ~size_t(255);
 constexpr size_t kOffHubSeq = kOffHub + (size_t)kHubCap * sizeof(PhHub);
-constexpr size_t kOffSettled = (kOffHubSeq + (size_t)kHubCap * 4 + 255) & ~size_t(255);
-constexpr size_t kSettledBytes = (size_t)ADDS_NOALLOC_MAX_N / 8; /* one bit per vertex */
-constexpr size_t kOffPool = (kOffSettled + kSettledBytes + 4095) & ~size_t(4095);
+constexpr size_t kOffPool = (kOffHubSeq + (size_t)kHubCap * 4 + 4095) & ~size_t(4095);
 constexpr size_t kEnd = kOffPool + (size_t)kPages * PH_PAGE * 8;
 static_assert(sizeof(PhGlobal) <= kOffGrp, "control block does not fit");
 static_assert(sizeof(PhGroup) <= kOffQd - kOffGrp, "group state does not fit");
@@ -189,8 +187,8 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
     void *p = nullptr;
     NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     int bps_i = 0, bps_f = 0, sms = 0;
-    NA_CK(adds_phase_prepare(false, kVariant, false, &bps_i));
-    NA_CK(adds_phase_prepare(true, kVariant, false, &bps_f));
+    NA_CK(adds_phase_prepare(false, kVariant, &bps_i));
+    NA_CK(adds_phase_prepare(true, kVariant, &bps_f));
     NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bps = bps_i < bps_f ? bps_i : bps_f;
     if (bps < 1) return ADDS_ERR_UNSUPPORTED;
@@ -206,7 +204,6 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   unsigned long long *pt = (unsigned long long *)(B + kOffPt);
   PhHub *hub = (PhHub *)(B + kOffHub);
   unsigned *hub_seq = (unsigned *)(B + kOffHubSeq);
-  unsigned *settled = (unsigned *)(B + kOffSettled); /* cleared by the solve's INIT phase */
   unsigned long long *pool = (unsigned long long *)(B + kOffPool);
 
   /* clear the state that must start at zero (the array keeps the previous
@@ -229,7 +226,6 @@ extern "C" int adds_sssp_noalloc(uint32_t n, uint64_t m, const uint32_t *row_sta
   desc.edges = (const uint2 *)edges;
   desc.split = nullptr; /* the weight-sorted copy would need memory */
   desc.dist = dist;
-  desc.settled = settled;
   desc.n = n;
   desc.src = src;
   desc.m = m;

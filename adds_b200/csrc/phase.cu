@@ -67,18 +67,6 @@ __device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
 __device__ __forceinline__ void red_min(unsigned *p, unsigned v) {
   asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ void red_or(unsigned *p, unsigned v) {
-  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-/* settled-filter word, cached in L1: the hub vertices most edges point at
- * share a few words.  L1 is not coherent with other SMs' red.or, so a word
- * may read a bit as still clear; that only costs the gather the bit would
- * have saved (bits are never cleared within a launch's query). */
-__device__ __forceinline__ unsigned ld_ca32(const unsigned *p) {
-  unsigned v;
-  asm("ld.global.ca.u32 %0, [%1];" : "=r"(v) : "l"(p));
-  return v;
-}
 /* Edge stream load: read-only path, no L1 allocation.  An L2 evict_first
  * hint on these loads measured 2.6 % slower on R-MAT 24 (5.85 vs 5.70 ms):
  * a row's edges are often read again by the next light/heavy phase. */
@@ -86,48 +74,6 @@ __device__ __forceinline__ uint2 ld_edge(const uint2 *p) {
   uint2 r;
   asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
   return r;
-}
-
-/* bulk-copy staging (PTX ISA: mbarrier, cp.async.bulk).  One mbarrier per
- * CTA counts one arrival (thread 0) plus the bytes of every copy; the
- * copies go to this CTA's own shared memory, never with multicast. */
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0u;
-}
-/* 1-D bulk copy global -> this CTA's shared memory; both addresses and the
- * size are multiples of 16 bytes */
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
-                                         unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-/* generic-proxy accesses of shared memory before async-proxy writes to it */
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 enum : unsigned { W_BARRIER = 1, W_PT = 2, W_ALLOC = 3, W_MAPPING = 4, W_HUB = 5, W_COPY = 6 };
@@ -215,19 +161,7 @@ struct PSmem {
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
   unsigned hub_made; /* this CTA cut a row into records in the current phase */
   unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
-  /* bulk-copy staging of split-row chunks (tma_rows): the mbarrier, its
-   * phase parity, and whether the chunk's edges are in shared memory */
-  unsigned long long tma_bar;
-  unsigned tma_par, ck_tma;
 };
-
-/* the staging area of the bulk copies: PH_TMA_BYTES of dynamic shared
- * memory past PSmem (present only in launches with tma_rows) */
-template <int BLOCK, int UU>
-__device__ __forceinline__ uint2 *tma_buf(PSmem<BLOCK, UU> &S) {
-  return reinterpret_cast<uint2 *>(reinterpret_cast<unsigned char *>(&S) +
-                                   ((sizeof(PSmem<BLOCK, UU>) + 15u) & ~(size_t)15u));
-}
 
 /* what a CTA keeps for the kernel's lifetime; the group's arrays are
  * recomputed from the parameters where they are used */
@@ -474,9 +408,6 @@ __device__ __forceinline__ void entry_item(const PhParams &P, Ctx &c, PSmem<BLOC
     ++nrepush;
     return;
   }
-  /* v's distance is at or below the bucket being settled: mark it for the
-   * settled filter (a heavy entry was marked when its light phase ran) */
-  if (mode == PH_M_LIGHT && Q.settled) red_or(Q.settled + (v >> 5), 1u << (v & 31u));
   const unsigned r0 = __ldg(Q.row + v), r1 = __ldg(Q.row + v + 1);
   const unsigned nl = (Q.split && !S.D.full) ? __ldg(Q.split + v) : (r1 - r0);
   if (mode == PH_M_LIGHT) {
@@ -547,7 +478,6 @@ __device__ __forceinline__ void finish_items(PSmem<BLOCK, UU> &S, unsigned k, un
     S.it_off[EPT * BLOCK] = tot;
     S.ck_k = k;
     S.ck_E = tot;
-    S.ck_tma = 0u; /* frontier chunks read the edge array directly */
   }
   __syncthreads();
 }
@@ -678,10 +608,7 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
  * false when no record is left.  Every thread calls it. */
 template <bool FLT, int BLOCK, int UU>
 __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
-  /* with bulk-copy staging a claim takes as many records as the staging
-   * area holds */
-  const unsigned K = P.tma_rows ? min(PH_TMA_REC, PH_HUB_PER_CLAIM(BLOCK))
-                                : PH_HUB_PER_CLAIM(BLOCK);
+  constexpr unsigned K = PH_HUB_PER_CLAIM(BLOCK);
   const unsigned tid = threadIdx.x;
   PhGroup *G = grp_of(P, c);
   const PhQuery &Q = P.qs[S.D.q];
@@ -733,18 +660,6 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
         rb = h.z;
         re = h.w;
         du = h.y;
-        if (P.tma_rows) {
-          /* stage the chunk in this CTA's shared memory: edge indices
-           * widened to even (16-byte boundaries; the edge array is padded
-           * past m); the item then indexes the staging slot */
-          const unsigned e0 = h.z & ~1u, e1 = (h.w + 1u) & ~1u;
-          uint2 *slot = tma_buf(S) + tid * PH_TMA_EDGES;
-          fence_proxy_async_smem();
-          mbar_expect_tx(&S.tma_bar, (e1 - e0) * 8u);
-          bulk_g2s(slot, Q.edges + e0, (e1 - e0) * 8u, &S.tma_bar);
-          rb = tid * PH_TMA_EDGES + (h.z - e0);
-          re = rb + (h.w - h.z);
-        }
       } else {
         stale = true;
       }
@@ -753,32 +668,6 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
   S.it_rb[tid] = rb;
   S.it_du[tid] = du;
   const unsigned nstale = __syncthreads_count(stale);
-  if (P.tma_rows) {
-    /* every expected byte count is registered: one arrival completes the
-     * phase once the copies have landed.  The wait is bounded; on a
-     * timeout the error word is set and the chunk is dropped (the solve
-     * ends with the error) */
-    if (tid == 0) mbar_arrive(&S.tma_bar);
-    const unsigned par = S.tma_par;
-    bool done = false;
-    for (unsigned it = 0; it < (1u << 22); ++it) {
-      if (mbar_try_wait(&S.tma_bar, par)) {
-        done = true;
-        break;
-      }
-      if ((it & 1023u) == 1023u && gtimer() > c.deadline) break;
-    }
-    if (!done) {
-      raise_err(P.g, PH_ERR_TIMEOUT, W_COPY);
-      rb = re = 0u;
-      S.it_rb[tid] = 0u;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      S.tma_par = par ^ 1u;
-      S.ck_tma = 1u;
-    }
-  }
   if (tid == 0) {
     S.st_stale += nstale;
     S.st_hubs += k - nstale;
@@ -790,7 +679,6 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
     S.it_off[BLOCK] = tot;
     S.ck_k = k;
     S.ck_E = tot;
-    S.ck_tma = P.tma_rows ? 1u : 0u;
   }
   __syncthreads();
   return true;
@@ -817,8 +705,6 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   const float scale = Q.scale;
   const unsigned shift = Q.shift;
   const unsigned *off = S.it_off; /* off[k] = E */
-  const bool staged = S.ck_tma != 0u; /* split-row chunk edges in shared memory */
-  const uint2 *tb = tma_buf(S);
   unsigned lo = 0; /* item of the thread's last edge: its edges only move forward */
   uint2 ne[U];
   unsigned nu[U];
@@ -843,8 +729,7 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
       ne[u] = make_uint2(0u, 0u);
       if (e < E) {
         find(e);
-        ne[u] = staged ? tb[S.it_rb[lo] + (e - off[lo])]
-                       : ld_edge(edges + S.it_rb[lo] + (e - off[lo]));
+        ne[u] = ld_edge(edges + S.it_rb[lo] + (e - off[lo]));
         nu[u] = S.it_du[lo];
       }
     }
@@ -852,7 +737,6 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   const unsigned mine = warp * 32u * U + lane; /* offset of the thread's first edge */
   if (nit) load_round(mine);
   unsigned nedges = 0;
-  const unsigned *settled = Q.settled;
   for (unsigned it = 0; it < nit; ++it) {
     unsigned dst[U], nd[U], cur[U], bk[U];
 #pragma unroll
@@ -868,19 +752,6 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
       }
     }
     if (it + 1u < nit) load_round((it + 1u) * R + mine);
-    /* settled filter: a new distance in a later bucket than the one being
-     * settled cannot improve a vertex whose bit is set (its distance is in
-     * that bucket or below, and buckets order distances), so neither the
-     * gather nor the relaxation happens */
-    if (settled) {
-      unsigned sw[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        sw[u] = (nd[u] != 0xFFFFFFFFu && bk[u] > base) ? ld_ca32(settled + (dst[u] >> 5)) : 0u;
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        if ((sw[u] >> (dst[u] & 31u)) & 1u) nd[u] = 0xFFFFFFFFu;
-    }
 #pragma unroll
     for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
     /* an improvement on the gathered value is applied with a reduction (no
@@ -929,40 +800,60 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
     } else {
       for (unsigned i = rank * BLOCK + tid; i < Q.n; i += gsize * BLOCK) __stcg(Q.dist + i, inf);
     }
-    if (Q.settled) {
-      const unsigned nw = (Q.n + 31u) >> 5;
-      for (unsigned i = rank * BLOCK + tid; i < nw; i += gsize * BLOCK) __stcg(Q.settled + i, 0u);
-    }
     return;
   }
   if (mode == PH_M_SCAN) {
-    /* a dense bucket: every vertex whose distance lies in it goes to NEXT,
-     * once, with its current distance.  Tiles of 4 x BLOCK vertices are
-     * dealt round-robin over the group's CTAs (one 16-byte load per thread);
-     * nothing relaxes in this phase, so the distances do not move. */
+    /* A scan over the distances.  Light scan (list = the bucket's slot):
+     * every vertex whose distance lies in the bucket goes to NEXT, once,
+     * with its current distance.  Heavy scan (list = SETTLED): every vertex
+     * of the settled bucket that has heavy edges goes to SETTLED, in vertex
+     * order, so the heavy phase reads their rows in address order and pops
+     * no duplicates.  Nothing relaxes in this phase, so the distances do not
+     * move.  A CTA takes tiles of 4 x BLOCK vertices round-robin, SCANG of
+     * them per round with all their 16-byte loads issued first; each tile's
+     * matches are staged (at most 4 x BLOCK) before the flush check, which
+     * the staging buffer's size allows. */
+    constexpr unsigned SCANG = 4;
+    const bool heavy = S.D.list == PH_LSETTLED;
+    const unsigned target = heavy ? PH_LSETTLED : PH_LNEXT;
     const unsigned base = S.D.base, n = Q.n;
     const unsigned inf = P.is_float ? 0x7F7FFFFFu : 0x7FFFFFFFu;
     const bool vec = (reinterpret_cast<unsigned long long>(Q.dist) & 15ull) == 0ull;
     const unsigned ntile = (n + 4u * BLOCK - 1u) / (4u * BLOCK);
-    for (unsigned t = solo ? 0u : c.rank; t < ntile; t += solo ? 1u : P.gsize) {
-      const unsigned v0 = t * 4u * BLOCK + 4u * tid;
-      unsigned d[4];
-      if (vec && v0 + 3u < n) {
-        const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(Q.dist + v0));
-        d[0] = x.x;
-        d[1] = x.y;
-        d[2] = x.z;
-        d[3] = x.w;
-      } else {
+    const unsigned r0 = solo ? 0u : c.rank, stride = solo ? 1u : P.gsize;
+    for (unsigned t0 = r0; t0 < ntile; t0 += SCANG * stride) {
+      unsigned d[SCANG][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) d[j] = (v0 + j < n) ? __ldcg(Q.dist + v0 + j) : inf;
+      for (unsigned g = 0; g < SCANG; ++g) {
+        const unsigned t = t0 + g * stride;
+        const unsigned v0 = t * 4u * BLOCK + 4u * tid;
+        if (t < ntile && vec && v0 + 3u < n) {
+          const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(Q.dist + v0));
+          d[g][0] = x.x;
+          d[g][1] = x.y;
+          d[g][2] = x.z;
+          d[g][3] = x.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            d[g][j] = (t < ntile && v0 + j < n) ? __ldcg(Q.dist + v0 + j) : inf;
+        }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (d[j] != inf && bucket_of<FLT>(d[j], Q.scale, Q.shift) == base)
-          stage<BLOCK, UU>(S, v0 + j, d[j], PH_LNEXT);
-      __syncthreads();
-      if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+      for (unsigned g = 0; g < SCANG; ++g) {
+        const unsigned v0 = (t0 + g * stride) * 4u * BLOCK + 4u * tid;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          bool take = d[g][j] != inf && bucket_of<FLT>(d[g][j], Q.scale, Q.shift) == base;
+          if (take && heavy) {
+            const unsigned v = v0 + j;
+            take = __ldg(Q.split + v) < __ldg(Q.row + v + 1) - __ldg(Q.row + v);
+          }
+          if (take) stage<BLOCK, UU>(S, v0 + j, d[g][j], target);
+        }
+        __syncthreads();
+        if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+      }
     }
     flush<BLOCK, UU>(P, c, S);
     return;
@@ -1059,6 +950,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       st_rlx64(&G->lh_prev, 0ull);
       st_rlx64(&G->dmask, 0ull);
       st_rlx64(&G->fmask, 0ull);
+      st_rlx32(&G->hs_block, 0u);
       __threadfence();
     }
     __syncwarp();
@@ -1097,16 +989,33 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         const unsigned k = ld_rlx32(&G->lh_k);
         full = k == 0u ? ld_rlx32(&G->lh_full) : (few ? 1u : 0u);
         if (lane == 0) {
+          if (full) st_rlx32(&G->hs_block, 1u);
           if (k == 1u && !few) st_rlx32(&G->lh_dense, 1u);
           st_rlx64(&G->lh_prev, tn - hn);
           st_rlx32(&G->lh_k, k + 1u);
         }
       }
     } else if (ts > hs) {
-      mode = PH_M_HEAVY;
-      list = PH_LSETTLED;
-      lo = hs;
-      hi = ts;
+      /* a large settled list (duplicates included) is rebuilt once by a
+       * heavy scan: each settled vertex with heavy edges once, in vertex
+       * order; the list's entries are dropped */
+      const PhQuery &Qh = P.qs[q];
+      const unsigned long long thr = max(4096u, Qh.n >> (P.dense_shift ? P.dense_shift : 31u));
+      if (P.dense_shift && Qh.split && ts - hs > thr && ld_rlx32(&G->hs_block) == 0u) {
+        mode = PH_M_SCAN;
+        list = PH_LSETTLED;
+        lo = 0ull;
+        hi = Qh.n;
+        if (lane == 0) {
+          st_rlx64(&G->head[PH_LSETTLED], ts);
+          st_rlx32(&G->hs_block, 1u);
+        }
+      } else {
+        mode = PH_M_HEAVY;
+        list = PH_LSETTLED;
+        lo = hs;
+        hi = ts;
+      }
     } else if (P.near_far) {
       /* near-far: the threshold moves up one bucket, or to the smallest
        * bucket pushed to the far pile since it last moved, and the pile is
@@ -1168,6 +1077,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
           st_rlx32(&G->lh_full, ld_rlx32(&G->lh_dense) != 0u ? 0u : 1u);
           st_rlx32(&G->lh_dense, 0u);
           st_rlx32(&G->lh_k, 0u);
+          st_rlx32(&G->hs_block, 0u);
         }
       } else if (ma | mb) {
         /* the nearest non-empty slot; with adaptation on, while the entries
@@ -1207,6 +1117,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         mode = PH_M_LIGHT;
         base += top;
         if (lane == 0) st_rlx32(&G->base, base);
+        bool hsb = nx != 0u;
         if (P.lh_adapt) {
           /* a new bucket: whole rows unless the last bucket was dense */
           full = ld_rlx32(&G->lh_dense) != 0u ? 0u : 1u;
@@ -1215,7 +1126,9 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
             st_rlx64(&G->lh_prev, cum);
             st_rlx32(&G->lh_k, 1u);
           }
+          hsb = hsb || full != 0u;
         }
+        if (lane == 0) st_rlx32(&G->hs_block, hsb ? 1u : 0u);
       } else {
         next_query = true;
       }
@@ -1382,12 +1295,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     S.st_hubs = S.st_solo = 0;
     S.tr_e = S.tr_mi = S.tr_mp = 0ull;
     for (int i = 0; i < 8; ++i) S.cy[i] = 0ull;
-    S.ck_tma = 0u;
-    S.tma_par = 0u;
-    if (P.tma_rows) {
-      mbar_init(&S.tma_bar, 1u);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
   }
   if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
@@ -1501,22 +1408,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   }
 }
 
-/* dynamic shared memory of a launch: PSmem, plus the bulk-copy staging
- * area when split-row chunks are staged (tma_rows) */
-template <int BLOCK, int MINB>
-static size_t smem_bytes(bool tma) {
-  const size_t s = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
-  return tma ? ((s + 15u) & ~(size_t)15u) + PH_TMA_BYTES : s;
-}
-
 template <bool FLT, int BLOCK, int MINB>
-static cudaError_t prep_one(bool tma, int *max_blocks_per_sm) {
+static cudaError_t prep_one(int *max_blocks_per_sm) {
+  const size_t smem = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
   cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_bytes<BLOCK, MINB>(true));
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      max_blocks_per_sm, phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem_bytes<BLOCK, MINB>(tma));
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
+                                                       phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
 }
 
 template <bool FLT, int BLOCK, int MINB>
@@ -1526,7 +1425,7 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P.groups * P.gsize);
   cfg.blockDim = dim3(BLOCK);
-  cfg.dynamicSmemBytes = smem_bytes<BLOCK, MINB>(P.tma_rows != 0u);
+  cfg.dynamicSmemBytes = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -1600,11 +1499,10 @@ int adds_phase_variant_block(int variant) {
   return 0;
 }
 
-cudaError_t adds_phase_prepare(bool flt, int variant, bool tma, int *max_blocks_per_sm) {
+cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm) {
   using namespace adds_phase;
 #define X(i, b, m) \
-  if (variant == i) \
-    return flt ? prep_one<true, b, m>(tma, max_blocks_per_sm) : prep_one<false, b, m>(tma, max_blocks_per_sm);
+  if (variant == i) return flt ? prep_one<true, b, m>(max_blocks_per_sm) : prep_one<false, b, m>(max_blocks_per_sm);
   PH_VARIANTS(X)
 #undef X
   return cudaErrorInvalidValue;
@@ -1662,8 +1560,8 @@ int ph_engine_upload(PhEngine &E, cudaStream_t st) {
   return 0;
 }
 
-static int ph_blocks_per_sm(bool flt, int variant, bool tma, int *bps) {
-  return adds_phase_prepare(flt, variant, tma, bps) == cudaSuccess ? 0 : -5;
+static int ph_blocks_per_sm(bool flt, int variant, int *bps) {
+  return adds_phase_prepare(flt, variant, bps) == cudaSuccess ? 0 : -5;
 }
 
 /* Sizes the per-group pools for the largest query (x grow) and allocates. */
@@ -1676,8 +1574,7 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
   E.variant = (unsigned)k.variant;
   E.block = (unsigned)adds_phase_variant_block(k.variant);
   int bps = 0;
-  E.tma = k.tma_rows ? 1u : 0u;
-  if (E.block == 0 || ph_blocks_per_sm(flt, k.variant, E.tma != 0u, &bps) || bps < 1)
+  if (E.block == 0 || ph_blocks_per_sm(flt, k.variant, &bps) || bps < 1)
     return -9; /* ADDS_ERR_UNSUPPORTED */
   if (cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
     return -5;
@@ -1758,8 +1655,7 @@ int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery
 
 unsigned ph_hub_chunk(const PhKnobs &k) {
   const unsigned thr = std::max(64u, k.hub_threshold);
-  const unsigned c = std::max(64u, std::min(k.hub_chunk, thr));
-  return k.tma_rows ? std::min(c, PH_TMA_CHUNK) : c; /* a staging slot holds 256 edges */
+  return std::max(64u, std::min(k.hub_chunk, thr));
 }
 
 int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, PhParams *P) {
@@ -1786,8 +1682,6 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->lh_adapt = k.lh_adapt;
   P->near_far = k.near_far ? 1u : 0u;
   P->dense_shift = k.near_far ? 0u : k.dense_shift;
-  P->tma_rows = (k.tma_rows && E.tma) ? 1u : 0u;
-  if (k.tma_rows && !E.tma) return -9; /* engine sized without the staging area */
   P->is_float = E.flt ? 1u : 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;

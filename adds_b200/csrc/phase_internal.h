@@ -55,12 +55,6 @@ struct PhQuery {
                             split != NULL                                     */
   const unsigned *split; /* light edges (w < delta) at the start of each row  */
   unsigned *dist;        /* n distance words                                  */
-  /* settled filter, ceil(n/32) words or NULL: bit v set => bucket(dist[v])
-   * is at or below the bucket being settled (set when v is expanded from its
-   * bucket; both only move one way within a solve).  A relaxation whose new
-   * distance lands above the current bucket cannot improve such a vertex,
-   * so it is skipped without gathering dist[v]. */
-  unsigned *settled;
   unsigned n;
   unsigned src;
   float scale;           /* float graphs: key = floor(d * scale)              */
@@ -134,7 +128,11 @@ struct __align__(128) PhGroup {
   unsigned far_min;
   /* first light phase of a bucket opened by a scan: whole rows or not */
   unsigned lh_full;
-  unsigned pad5[14];
+  /* the settled list of the current bucket may not be rebuilt by a heavy
+   * scan: it was already, or a light phase relaxed whole rows, or the
+   * bucket was widened over several slots */
+  unsigned hs_block;
+  unsigned pad5[13];
   /* dense bucket slots (bit per slot): a slot whose pushes passed the dense
    * threshold stops storing entries; its bucket is collected by a scan of
    * the distances when it opens (PH_M_SCAN) */
@@ -203,10 +201,6 @@ struct PhParams {
   unsigned dense_shift;        /* a bucket slot that receives more than
                                   max(n >> dense_shift, 4096) pushes turns
                                   dense (collected by a scan); 0 = never      */
-  unsigned tma_rows;           /* split-row chunks staged into shared memory
-                                  by bulk copies (cp.async.bulk) before they
-                                  are expanded; the launch then carries
-                                  PH_TMA_BYTES more dynamic shared memory    */
   unsigned is_float;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
@@ -224,7 +218,6 @@ struct PhEngine {
   bool flt = false;
   unsigned nq = 0, groups = 0, gsize = 0, block = 0, variant = 0;
   int req_group = 0; /* group_ctas knob the engine was sized with */
-  unsigned tma = 0;  /* sized for the bulk-copy record staging */
   unsigned pages_per_group = 0, ptn_log2 = 0, hub_cap = 0, max_n = 0;
   unsigned hub_eff = 0; /* split-row chunk length the record store is sized for */
   PhGroup *grp = nullptr;
@@ -250,21 +243,13 @@ struct PhKnobs {
   unsigned hub_threshold, hub_chunk, solo_max, adapt, lh_adapt;
   unsigned near_far;  /* near-far schedule instead of the bucket ring          */
   unsigned dense_shift; /* dense bucket slots (PhParams::dense_shift), 0 = off  */
-  unsigned tma_rows;    /* bulk-copy staging of split-row chunks (PhParams)   */
   unsigned long long timeout_ns;
 };
 
-/* bulk-copy staging of split-row chunks: records per claim, and edges per
- * record slot (a chunk of at most 256 edges, widened to even edge indices
- * so that every copy starts and ends on a 16-byte boundary) */
-#define PH_TMA_REC 8u
-#define PH_TMA_EDGES 258u
-#define PH_TMA_CHUNK 256u
-#define PH_TMA_BYTES (PH_TMA_REC * PH_TMA_EDGES * 8u)
 
 /* phase.cu host API (C++ linkage) */
 int adds_phase_variant_block(int variant);
-cudaError_t adds_phase_prepare(bool flt, int variant, bool tma, int *max_blocks_per_sm);
+cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm);
 cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st);
 int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery> &qv,
                     const PhKnobs &k, unsigned grow, cudaStream_t st);

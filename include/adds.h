@@ -101,12 +101,7 @@ typedef struct adds_opts {
                             them, and its bucket is collected by one pass over
                             the distances when it opens (no duplicate or stale
                             entries); 0 = auto (6), < 0 = off                */
-  int32_t tma_rows;      /* phase engine, 1: split-row chunks are staged into
-                            shared memory by bulk copies (cp.async.bulk, with
-                            an mbarrier) before they are expanded, instead of
-                            direct loads; chunks are then at most 256 edges;
-                            0 = direct loads                                */
-  int32_t reserved[2];
+  int32_t reserved[3];
 } adds_opts;
 
 /* Engines.  PHASE settles the buckets in bulk-synchronous phases (light

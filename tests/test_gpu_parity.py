@@ -209,7 +209,7 @@ def test_dense_bucket_scan(dense, lh, adapt):
     dg = A.Graph.from_csr(g)
     try:
         dg.trace(1 << 16)
-        d, st = dg.sssp(src, A.default_opts(**OPTS, engine=PHASE, delta_shift=8, light_heavy=lh,
+        d, st = dg.sssp(src, A.default_opts(**OPTS, engine=PHASE, delta_shift=10, light_heavy=lh,
                                             adapt=adapt, dense_scan=dense))
         tr, n = dg.trace_read(1 << 16)
         dg.trace(0)
@@ -225,21 +225,6 @@ def test_dense_bucket_scan(dense, lh, adapt):
     f = G.grid(128, 96, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=25)
     _check(f, 48 * 128 + 64, engine=PHASE, delta_shift=14, light_heavy=lh, adapt=adapt,
            dense_scan=dense)
-
-
-@pytest.mark.parametrize("variant", VARIANTS)
-@pytest.mark.parametrize("lh", [0, 2])
-def test_split_rows_staged_by_bulk_copies(variant, lh):
-    """tma_rows 1: split-row chunks reach shared memory by cp.async.bulk
-    (mbarrier-completed) before their edges are relaxed; the distances stay
-    the oracle's (int R-MAT with many split rows, float grid)."""
-    g = G.rmat(14, 16, seed=28, w_hi=10000)
-    st = _check(g, G.max_degree_vertex(g), engine=PHASE, tma_rows=1, hub_threshold=64,
-                light_heavy=lh, block_threads=variant[0], ctas_per_sm=variant[1])
-    assert st["hub_chunks"] > 0
-    f = G.grid(96, 80, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=29)
-    _check(f, 40 * 96 + 48, engine=PHASE, tma_rows=1, hub_threshold=64, light_heavy=lh,
-           block_threads=variant[0], ctas_per_sm=variant[1])
 
 
 @pytest.mark.parametrize("ctas", [1, 16, 64])
