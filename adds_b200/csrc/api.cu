@@ -1020,9 +1020,9 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   }
   k->group_ctas = o->group_ctas > 0 ? o->group_ctas : (t->group_ctas > 0 ? t->group_ctas : 0);
   k->solo_max = o->solo_max >= 0 ? o->solo_max : (t->solo_max >= 0 ? t->solo_max : 1024);
-  /* dense bucket slots: explicit > tuned > 6 (a slot holding more than n/64
-   * pushes is cheaper to collect with one pass over the distances) */
-  k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : 6);
+  /* dense bucket slots: explicit > tuned > off (measured on R-MAT 24: the
+   * scans remove the stale entries but cost as much as they save) */
+  k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : -1);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -2071,7 +2071,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
     try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
     try_field(&adds_opts::light_heavy, {0, 1, 2});
     try_field(&adds_opts::adapt, {0, 1});
-    try_field(&adds_opts::dense_scan, {-1, 4, 8});
+    try_field(&adds_opts::dense_scan, {4, 6, 8});
     /* fewer CTAs for graphs whose phases are too short to use the GPU */
     if (g->m < (1ull << 24)) try_field(&adds_opts::group_ctas, {16, 32, 64, 148});
     if (cur.delta_shift != s0) {

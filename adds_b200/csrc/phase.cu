@@ -1325,8 +1325,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
         ++nphase;
         if (!solo_ok<BLOCK, UU>(P, S)) break;
         if (tid == 0) {
-          st_rlx32(&G->producers, 1u); /* this CTA alone expands the phase */
-          __threadfence();
+          /* this CTA alone expands the phase; no fence: until the group is
+           * released (with a fence) nothing outside this CTA reads what the
+           * solo phases write, and the CTA's barriers order its own accesses */
+          st_rlx32(&G->producers, 1u);
           ++S.st_solo;
           if (P.trace && c.gi == 0u) { /* mark the record just written as solo */
             const unsigned long long i = ld_rlx64(&P.g->st_trace) - 1ull;
@@ -1335,8 +1337,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
         }
         run_phase<FLT, BLOCK, UU>(P, c, S, true);
         if (tracing) trace_account<BLOCK, UU>(P, c, S);
-        __syncthreads();
-        if (tid == 0) __threadfence();
         __syncthreads();
       }
       if (tid == 0) {

@@ -100,7 +100,8 @@ typedef struct adds_opts {
                             max(n >> dense_scan, 4096) pushes stops storing
                             them, and its bucket is collected by one pass over
                             the distances when it opens (no duplicate or stale
-                            entries); 0 = auto (6), < 0 = off                */
+                            entries); 0 = auto (off unless tuned), < 0 = off,
+                            6 = n/64                                        */
   int32_t reserved[3];
 } adds_opts;
 
