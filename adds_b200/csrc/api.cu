@@ -2009,102 +2009,99 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
     o.adapt = k.adapt;
     return o;
   };
-  /* in: the engine to tune; auto times both and tunes the faster one (the
-   * phase engine wins on low-diameter graphs, the asynchronous one where
-   * thousands of buckets each hold a thin frontier) */
-  const int want = (best && best->engine > 0) ? best->engine : ADDS_ENGINE_AUTO;
-  adds_opts cur = defaults(want == ADDS_ENGINE_ASYNC ? ADDS_ENGINE_ASYNC : ADDS_ENGINE_PHASE);
-  double bm = time_solves(g, srcs, ns, &cur);
-  if (want == ADDS_ENGINE_AUTO) {
-    const adds_opts alt = defaults(ADDS_ENGINE_ASYNC);
-    const double ma = time_solves(g, srcs, ns, &alt);
-    if (ma < bm) {
-      bm = ma;
-      cur = alt;
-    }
-    /* small graphs: the phase engine on fewer CTAs (cheaper barriers) is a
-     * candidate of its own before the engine is chosen */
-    if (g->m < (1ull << 24)) {
-      for (int gc : {16, 32, 64}) {
-        adds_opts t = defaults(ADDS_ENGINE_PHASE);
-        t.group_ctas = gc;
+  /* Coordinate descent of one engine's knobs from a start point; returns the
+   * best options found and their time. */
+  auto descend = [&](adds_opts cur, double bm, adds_opts *out) {
+    resolve(g, &cur, &k, &s0, &sc); /* knobs of the engine */
+    auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
+      for (int v : vals) {
+        if (v == cur.*f) continue;
+        adds_opts t = cur;
+        t.*f = v;
         const double ms = time_solves(g, srcs, ns, &t);
-        if (ms < bm) {
+        if (ms < bm * 0.98) {
           bm = ms;
           cur = t;
         }
       }
-    }
-  }
-  resolve(g, &cur, &k, &s0, &sc); /* knobs of the chosen engine */
-  auto try_field = [&](int32_t adds_opts::*f, const std::vector<int> &vals) {
-    for (int v : vals) {
-      if (v == cur.*f) continue;
-      adds_opts t = cur;
-      t.*f = v;
-      const double ms = time_solves(g, srcs, ns, &t);
-      if (ms < bm * 0.98) {
-        bm = ms;
-        cur = t;
+    };
+    std::vector<int> shifts;
+    for (int d = -4; d <= 4; ++d)
+      if (s0 + d >= 0 && s0 + d <= 31) shifts.push_back(s0 + d);
+    try_field(&adds_opts::delta_shift, shifts);
+    if (cur.engine == ADDS_ENGINE_PHASE) {
+      /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
+      const int combos[6][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}, {128, 8}};
+      for (const auto &cb : combos) {
+        adds_opts t = cur;
+        t.block_threads = cb[0];
+        t.ctas_per_sm = cb[1];
+        if (t.block_threads == cur.block_threads && t.ctas_per_sm == cur.ctas_per_sm) continue;
+        const double ms = time_solves(g, srcs, ns, &t);
+        if (ms < bm * 0.98) {
+          bm = ms;
+          cur = t;
+        }
       }
+      /* fewer CTAs for graphs whose phases are too short to use the GPU */
+      if (g->m < (1ull << 24)) try_field(&adds_opts::group_ctas, {8, 16, 32, 64, 148});
+      try_field(&adds_opts::solo_max, {0, 256, 512, 1024, 2048, 4096, 16384});
+      try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
+      try_field(&adds_opts::light_heavy, {0, 1, 2});
+      try_field(&adds_opts::adapt, {0, 1});
+      try_field(&adds_opts::dense_scan, {4, 6, 8});
+    } else {
+      try_field(&adds_opts::window, {1, 2, 3, 4, 8});
+      try_field(&adds_opts::batch_max, {64, 128, 256, 512});
+      try_field(&adds_opts::hub_threshold, {4096, 16384, 65536});
+      try_field(&adds_opts::block_threads, {128, 256, 512});
+      try_field(&adds_opts::greed, {0, 2, 4, 8});
+      int maxb = g->eng.max_bps[block_index(cur.block_threads > 0 ? cur.block_threads : 256)];
+      std::vector<int> cps;
+      for (int c = 1; c <= maxb; ++c) cps.push_back(c);
+      try_field(&adds_opts::ctas_per_sm, cps);
+      try_field(&adds_opts::strict_order, {0, 1});
+      try_field(&adds_opts::local_max, {0, 64, 256, 512});
+      try_field(&adds_opts::light_heavy, {0, 1});
     }
-  };
-  std::vector<int> shifts;
-  for (int d = -4; d <= 4; ++d)
-    if (s0 + d >= 0 && s0 + d <= 31) shifts.push_back(s0 + d);
-  try_field(&adds_opts::delta_shift, shifts);
-  if (cur.engine == ADDS_ENGINE_PHASE) {
-    /* kernel variant (threads per CTA x CTAs per SM), then the schedule */
-    const int combos[6][2] = {{256, 4}, {512, 2}, {1024, 1}, {256, 2}, {512, 1}, {128, 8}};
-    for (const auto &cb : combos) {
-      adds_opts t = cur;
-      t.block_threads = cb[0];
-      t.ctas_per_sm = cb[1];
-      if (t.block_threads == cur.block_threads && t.ctas_per_sm == cur.ctas_per_sm) continue;
-      const double ms = time_solves(g, srcs, ns, &t);
-      if (ms < bm * 0.98) {
-        bm = ms;
-        cur = t;
-      }
-    }
-    try_field(&adds_opts::solo_max, {0, 256, 512, 1024, 2048, 4096});
-    try_field(&adds_opts::hub_threshold, {128, 256, 1024, 4096});
-    try_field(&adds_opts::light_heavy, {0, 1, 2});
-    try_field(&adds_opts::adapt, {0, 1});
-    try_field(&adds_opts::dense_scan, {4, 6, 8});
-    /* fewer CTAs for graphs whose phases are too short to use the GPU */
-    if (g->m < (1ull << 24)) try_field(&adds_opts::group_ctas, {16, 32, 64, 148});
-    if (cur.delta_shift != s0) {
+    if (cur.delta_shift != s0) { /* second look around the new delta */
       std::vector<int> s2;
       for (int d = -1; d <= 1; ++d)
         if (cur.delta_shift + d >= 0 && cur.delta_shift + d <= 31) s2.push_back(cur.delta_shift + d);
       try_field(&adds_opts::delta_shift, s2);
     }
-    if (bm >= 1e29) return ADDS_ERR_DEVICE_TIMEOUT;
-    g->tuned_opts = cur;
-    g->tuned_opts.stream = nullptr;
-    g->tuned = 1;
-    if (best) *best = g->tuned_opts;
-    if (best_ms) *best_ms = bm / ns;
-    return ADDS_OK;
-  }
-  try_field(&adds_opts::window, {1, 2, 3, 4, 8});
-  try_field(&adds_opts::batch_max, {64, 128, 256, 512});
-  try_field(&adds_opts::hub_threshold, {4096, 16384, 65536});
-  try_field(&adds_opts::block_threads, {128, 256, 512});
-  try_field(&adds_opts::greed, {0, 2, 4, 8});
-  int maxb = g->eng.max_bps[block_index(cur.block_threads > 0 ? cur.block_threads : 256)];
-  std::vector<int> cps;
-  for (int c = 1; c <= maxb; ++c) cps.push_back(c);
-  try_field(&adds_opts::ctas_per_sm, cps);
-  try_field(&adds_opts::strict_order, {0, 1});
-  try_field(&adds_opts::local_max, {0, 64, 256, 512});
-  try_field(&adds_opts::light_heavy, {0, 1});
-  if (cur.delta_shift != s0) { /* second look around the new delta */
-    std::vector<int> s2;
-    for (int d = -1; d <= 1; ++d)
-      if (cur.delta_shift + d >= 0 && cur.delta_shift + d <= 31) s2.push_back(cur.delta_shift + d);
-    try_field(&adds_opts::delta_shift, s2);
+    *out = cur;
+    return bm;
+  };
+  /* in: the engine to tune; auto times both and tunes the faster one (the
+   * phase engine wins on low-diameter graphs, the asynchronous one where
+   * thousands of buckets each hold a thin frontier).  Small graphs (under
+   * 2^24 edges, where a solve takes well under a millisecond) get a full
+   * descent of both engines, since a start point does not predict the
+   * winner there (the phase engine on few CTAs needs its knobs first). */
+  const int want = (best && best->engine > 0) ? best->engine : ADDS_ENGINE_AUTO;
+  adds_opts cur = defaults(want == ADDS_ENGINE_ASYNC ? ADDS_ENGINE_ASYNC : ADDS_ENGINE_PHASE);
+  double bm = time_solves(g, srcs, ns, &cur);
+  if (want == ADDS_ENGINE_AUTO && g->m < (1ull << 24)) {
+    adds_opts bp, ba;
+    adds_opts p0 = cur;
+    p0.group_ctas = 32;
+    const double m0 = time_solves(g, srcs, ns, &p0);
+    const double mp = descend(m0 < bm ? p0 : cur, m0 < bm ? m0 : bm, &bp);
+    const adds_opts a0 = defaults(ADDS_ENGINE_ASYNC);
+    const double ma = descend(a0, time_solves(g, srcs, ns, &a0), &ba);
+    cur = mp <= ma ? bp : ba;
+    bm = mp <= ma ? mp : ma;
+  } else {
+    if (want == ADDS_ENGINE_AUTO) {
+      const adds_opts alt = defaults(ADDS_ENGINE_ASYNC);
+      const double ma = time_solves(g, srcs, ns, &alt);
+      if (ma < bm) {
+        bm = ma;
+        cur = alt;
+      }
+    }
+    bm = descend(cur, bm, &cur);
   }
   if (bm >= 1e29) return ADDS_ERR_DEVICE_TIMEOUT;
   g->tuned_opts = cur;

@@ -738,16 +738,14 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
   if (nit) load_round(mine);
   unsigned nedges = 0;
   for (unsigned it = 0; it < nit; ++it) {
-    unsigned dst[U], nd[U], cur[U], bk[U];
+    unsigned dst[U], nd[U], cur[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       dst[u] = ne[u].x;
       nd[u] = 0xFFFFFFFFu;
-      bk[u] = 0u;
       if (nu[u] != 0xFFFFFFFFu) {
         nd[u] = FLT ? __float_as_uint(__fadd_rn(__uint_as_float(nu[u]), __uint_as_float(ne[u].y)))
                     : nu[u] + ne[u].y;
-        bk[u] = bucket_of<FLT>(nd[u], scale, shift);
         ++nedges;
       }
     }
@@ -763,7 +761,8 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
     for (int u = 0; u < U; ++u) {
       if (nd[u] < cur[u]) {
         red_min(dist + dst[u], nd[u]);
-        stage<BLOCK, UU>(S, dst[u], nd[u], route(bk[u], base, P.near_far));
+        stage<BLOCK, UU>(S, dst[u], nd[u],
+                         route(bucket_of<FLT>(nd[u], scale, shift), base, P.near_far));
       }
     }
     if ((it % PSmem<BLOCK, UU>::SEGI) == PSmem<BLOCK, UU>::SEGI - 1u || it + 1u == nit) {

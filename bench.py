@@ -365,6 +365,14 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
                    "solves; host wall clock; the 4-byte source id is the step input, the "
                    "distance array the result"}
     work_edges = st["edges_scanned"]
+    # run-to-run spread: the timed steps again, one synchronous solve each
+    # (outside the timed region; per-solve device time of the kernel)
+    each = []
+    for s_ in steps:
+        _, st1 = g.sssp(s_, opts)
+        each.append(st1["kernel_ms"])
+    each_sorted = sorted(each)
+    med = statistics.median(each_sorted)
     if args.trace:  # one more solve with the phase trace on (outside the timed region)
         g.trace(1 << 16)
         g.sssp(steps[0], opts)
@@ -409,6 +417,9 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
                                                         "batch_max", "strict_order")}
                       if tuned else None),
             "tune_ms_per_solve": tune_ms,
+            "solve_kernel_ms_each": each,
+            "solve_kernel_ms_median": med,
+            "solve_kernel_ms_spread_pct": 100.0 * (each_sorted[-1] - each_sorted[0]) / med,
         },
     }
     if check_parity:
