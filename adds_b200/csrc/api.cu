@@ -372,6 +372,7 @@ static void fill_stats(const Engine &E, const EngParams &P, adds_stats *s) {
   s->batches = g.st_batches;
   s->hub_chunks = g.st_hub;
   s->hub_stale = g.st_hub_stale;
+  s->local_batches = g.st_local;
   s->heavy_lists = g.st_heavy;
   for (int i = 0; i < 6; ++i) s->phase_cycles[i] = g.st_cyc[i];
   s->mid_flush_cycles = g.st_pad[0];

@@ -61,6 +61,10 @@ __device__ __forceinline__ void st_rlx32(unsigned *p, unsigned v) {
 __device__ __forceinline__ void st_rel32(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+/* fire-and-forget atomic minimum (no result, so the thread does not wait) */
+__device__ __forceinline__ void red_min(unsigned *p, unsigned v) {
+  asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 /* where a wait gave up (GlobalCtl::err_where) */
 enum : unsigned {
@@ -125,12 +129,17 @@ __device__ void free_page(const EngParams &P, unsigned phys) {
   st_rlx64(&P.fq[t & P.fq_mask], ((unsigned long long)phys << 32) | (unsigned)t);
 }
 
-/* Marks cnt entries of page pi consumed; frees the page when all are. */
-__device__ __forceinline__ void consume(const EngParams &P, unsigned pi, unsigned cnt) {
+/* Marks cnt entries of page pi consumed and returns the count before; the
+ * caller frees the page (consume_end) when that completes it.  The two
+ * halves are split so that the wait for the count overlaps other work. */
+__device__ __forceinline__ unsigned consume_begin(const EngParams &P, unsigned pi, unsigned cnt) {
+  if (pi == PI_BAD || cnt == 0) return 0u;
+  return atomicAdd(&P.pcons[pi & 0x7FFFFFFFu], cnt);
+}
+__device__ __forceinline__ void consume_end(const EngParams &P, unsigned pi, unsigned cnt,
+                                            unsigned old) {
   if (pi == PI_BAD || cnt == 0) return;
-  const unsigned phys = pi & 0x7FFFFFFFu;
-  const unsigned old = atomicAdd(&P.pcons[phys], cnt);
-  if (old + cnt == ADDS_PAGE) free_page(P, phys);
+  if (old + cnt == ADDS_PAGE) free_page(P, pi & 0x7FFFFFFFu);
 }
 
 __device__ __forceinline__ unsigned long long *pt_cell(const QueryDesc &d, unsigned s,
@@ -168,16 +177,17 @@ __device__ bool slot_reserve(const EngParams &P, const QueryDesc &d, unsigned s,
                              unsigned long long *pbase, unsigned *pp0, unsigned *pp1,
                              unsigned long long *cvp, unsigned *cpi) {
   SlotCtr *sc = d.slots + s;
+  /* span of live entries the page-table ring must cover.  head is read
+   * together with the reservation (one round trip): a head older than the
+   * reservation only makes the span look longer, so the check stays safe.
+   * Claimers may also have moved head past this (still unwritten) range,
+   * whose entries they then wait for: head > base + c is legal and means a
+   * short span; the unsigned difference must not wrap into a spurious
+   * overflow. */
+  const unsigned long long head = ld_rlx64(&sc->head);
   const unsigned long long base = atomicAdd(&sc->tail, (unsigned long long)c);
   *pbase = base;
   *pp0 = *pp1 = PI_BAD;
-  /* span of live entries the page-table ring must cover.  head is read after
-   * the reservation: other CTAs may meanwhile have published later ranges
-   * and claimers may have moved head past this (still unwritten) range,
-   * whose entries they then wait for.  head > base + c is therefore legal
-   * and means a short span; the unsigned difference must not wrap into a
-   * spurious overflow. */
-  const unsigned long long head = ld_rlx64(&sc->head);
   const unsigned long long ptn = 1ull << d.ptn_log2;
   const unsigned long long end = base + c;
   if (end > head && end - head > (ptn - 3ull) * ADDS_PAGE) {
@@ -259,7 +269,11 @@ struct Smem {
   unsigned pcnt, total_edges, hub_chunks;
   unsigned cur_q, idle, hungry;
   unsigned loc_k, loc_slot, keep_slot;
-  unsigned hub_u, ptc_q;
+  unsigned hub_u, ptc_q, done_late;
+  /* descriptor of query qd_q, copied once per change of query, so that a
+   * batch reads its pointers from shared memory instead of HBM */
+  QueryDesc qd;
+  unsigned qd_q;
   /* page-table cache: last (virtual page -> page info) seen per slot of
    * query ptc_q.  A claimed or reserved entry keeps its page mapped, so a
    * hit on the same virtual page is always current. */
@@ -307,7 +321,16 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
                         unsigned long long deadline) {
   const unsigned lane = threadIdx.x & 31u;
   GlobalCtl *g = P.g;
-  if (ld_rlx32(&g->err) != 0u || ld_rlx32(&g->remaining) == 0u) {
+  /* independent control words are loaded together: a batch's acquisition
+   * is a chain of memory round trips, each one on a wave front's path */
+  const unsigned err0 = ld_rlx32(&g->err);
+  const unsigned rem0 = ld_rlx32(&g->remaining);
+  unsigned long long hh0 = 0ull, ht0 = 0ull;
+  if (lane == 0) {
+    hh0 = ld_rlx64(&g->hub_head);
+    ht0 = ld_rlx64(&g->hub_tail);
+  }
+  if (err0 != 0u || rem0 == 0u) {
     if (lane == 0) S.status = ST_EXIT;
     return;
   }
@@ -315,9 +338,9 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
   {
     unsigned long long ticket = ~0ull;
     if (lane == 0) {
-      unsigned long long hh = ld_rlx64(&g->hub_head);
+      unsigned long long hh = hh0;
       for (int tries = 0; tries < 4; ++tries) {
-        const unsigned long long ht = ld_rlx64(&g->hub_tail);
+        const unsigned long long ht = tries == 0 ? ht0 : ld_rlx64(&g->hub_tail);
         if (hh >= ht) break;
         const unsigned long long prev = atomicCAS(&g->hub_head, hh, hh + 1ull);
         if (prev == hh) { ticket = hh; break; }
@@ -364,10 +387,13 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
   unsigned q = S.cur_q;
   const unsigned tries = P.nq < 8u ? P.nq : 8u;
   for (unsigned t = 0; t < tries; ++t, q = (q + 1u == P.nq) ? 0u : q + 1u) {
-    const QueryDesc &d = P.qs[q];
+    /* the cached descriptor when it is this query's (shared memory) */
+    const QueryDesc &d = (q == S.qd_q) ? S.qd : P.qs[q];
     QueryCtl *ctl = d.ctl;
-    if (ld_rlx32(&ctl->done) != 0u) continue;
+    const unsigned qdone = ld_rlx32(&ctl->done);
     const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
+    const unsigned qshift = ld_rlx32(&ctl->shift);
+    if (qdone != 0u) continue;
     const unsigned base_b = (unsigned)ctrl & 0x7FFFFFFFu;
     const bool phase_h = ((unsigned)ctrl & ADDS_PHASE_H) != 0u;
     const unsigned base_key = (unsigned)(ctrl >> 32);
@@ -388,14 +414,19 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
       }
       continue;
     }
-    unsigned long long li = 0, hi = 0;
-    if (lane == 0) {
-      li = ld_rlx64(&lsc->inflight);
-      hi = ld_rlx64(&hsc->inflight);
-    }
-    li = __shfl_sync(0xFFFFFFFFu, li, 0);
-    hi = __shfl_sync(0xFFFFFFFFu, hi, 0);
+    /* the base slot's in-flight counts, read after its head and tail (a
+     * claimer raises them before it moves the head); needed only while the
+     * base bucket's light queue or heavy list looks empty */
     const bool strict = P.strict_order != 0u;
+    unsigned long long li = 0, hi = 0;
+    if (strict && ((lmask & hmask & 1u) == 0u)) {
+      if (lane == 0) {
+        li = ld_rlx64(&lsc->inflight);
+        hi = ld_rlx64(&hsc->inflight);
+      }
+      li = __shfl_sync(0xFFFFFFFFu, li, 0);
+      hi = __shfl_sync(0xFFFFFFFFu, hi, 0);
+    }
     const bool l_done = !(lmask & 1u) && (!strict || li == 0ull);
     const bool h_done = !(hmask & 1u) && (!strict || hi == 0ull);
     /* base-bucket state machine */
@@ -457,7 +488,7 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
       S.pi1 = pi1;
       S.base_b = (base_b + eff) & 0x7FFFFFFFu;
       S.base_key = base_key + eff;
-      S.shift = ld_rlx32(&ctl->shift);
+      S.shift = qshift;
       S.cur_q = q;
     }
     return;
@@ -476,15 +507,36 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
  * Every other slot gets one tail reservation and the entry stores; its
  * avail count is raised after the stores.  Replaces the per-warp match_any
  * + atomicAdd + st.cg + __threadfence + write_done update of push_work
- * (wl.h:1902-1928). */
+ * (wl.h:1902-1928).
+ *
+ * The flush that ends a batch also retires the batch: its done_k entries
+ * leave the live count and the in-flight count of done_slot (NO_SLOT for a
+ * split-row chunk).  The live count takes pushes minus done_k in one atomic
+ * before any entry is visible, so it never falls below what is queued or
+ * held.  When the CTA keeps entries of the batch's own slot, that slot's
+ * in-flight count takes kept minus done_k in one atomic (it stays at least
+ * the kept count, so the slot cannot retire under them); otherwise the
+ * batch leaves its slot after the new entries are published.  A flush that
+ * keeps every push publishes nothing and needs no fence. */
+#define NO_SLOT 0xFFFFFFFFu
 template <int BLOCK>
 __device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
-                      unsigned long long deadline, unsigned long long &st_pushes, bool keep) {
+                      unsigned long long deadline, unsigned long long &st_pushes, bool keep,
+                      unsigned done_k = 0u, unsigned done_slot = NO_SLOT) {
   const unsigned tid = threadIdx.x;
   const unsigned cnt = S.pcnt;
-  if (cnt == 0u) return; /* uniform: read after a barrier */
-  const unsigned qd = (unsigned)(&d - P.qs);
+  if (cnt == 0u) { /* uniform: read after a barrier */
+    if (tid == 0u && done_k) {
+      if (done_slot != NO_SLOT)
+        atomicAdd(&d.slots[done_slot].inflight, (unsigned long long)(0ull - done_k));
+      atomicSub(&d.ctl->live, done_k);
+    }
+    return;
+  }
+  const unsigned qd = S.q; /* d is this query's descriptor */
   const bool stale_cache = S.ptc_q != qd; /* uniform: read after a barrier */
+  /* whether CTAs are idle (keeps fewer entries local), read early */
+  const unsigned hungry = (keep && tid < 32u) ? ld_rlx32(&P.g->hungry) : 0u;
   if (tid < NSLOT) {
     S.hist[tid] = 0u;
     if (stale_cache) S.ptc_vp[tid] = ~0ull;
@@ -504,22 +556,30 @@ __device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
       const unsigned r = __ffs(rot) - 1u;
       if (r < P.window) {
         ks = (S.base_b + r) & (ADDS_NB - 1u);
-        const unsigned lmax = ld_rlx32(&P.g->hungry) ? P.local_max_hungry : P.local_max;
+        const unsigned lmax = hungry ? P.local_max_hungry : P.local_max;
         kn = min(min(__shfl_sync(0xFFFFFFFFu, c, ks), lmax), (unsigned)BLOCK);
       }
     }
+    const unsigned cg = c - ((tid == ks) ? kn : 0u);
+    const bool merged = kn != 0u && done_slot == ks;
     if (tid == 0u) {
-      atomicAdd(&d.ctl->live, cnt); /* count before any entry is visible */
-      __threadfence();
+      /* count before any entry is visible: the entries become visible
+       * through the avail increments below, each behind two barriers and a
+       * (cumulative) fence of the raising thread, which order this update
+       * before them as they order the entry stores */
+      if (cnt != done_k) atomicAdd(&d.ctl->live, cnt - done_k);
       st_pushes += cnt;
       S.keep_slot = kn ? ks : 0xFFFFFFFFu;
       S.loc_k = kn;
       S.loc_slot = ks;
+      S.done_late = (done_k != 0u && done_slot != NO_SLOT && !merged) ? 1u : 0u;
     }
     __syncwarp();
-    const unsigned cg = c - ((tid == ks) ? kn : 0u);
     S.gcnt[tid] = cg;
-    if (tid == ks && kn) atomicAdd(&d.slots[ks].inflight, (unsigned long long)kn);
+    if (tid == ks && kn) {
+      const unsigned long long add = merged ? (unsigned long long)kn - done_k : kn;
+      if (add) atomicAdd(&d.slots[ks].inflight, add);
+    }
     if (cg != 0u) {
       unsigned long long b;
       unsigned p0, p1;
@@ -564,7 +624,12 @@ __device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
     __threadfence();
     atomicAdd((unsigned long long *)&d.slots[tid].avail, (unsigned long long)S.gcnt[tid]);
   }
-  if (tid == 0u) S.pcnt = 0u;
+  if (tid == 0u) {
+    S.pcnt = 0u;
+    /* the batch leaves its slot after its pushes into that slot are
+     * reserved (the tail moved), so the slot is never seen empty between */
+    if (S.done_late) atomicAdd(&d.slots[done_slot].inflight, (unsigned long long)(0ull - done_k));
+  }
   __syncthreads();
 }
 
@@ -644,23 +709,31 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
     S.loc_k = 0;
     S.q = S.cur_q;
     S.ptc_q = 0xFFFFFFFFu;
+    S.qd_q = 0xFFFFFFFFu;
   }
   if (tid < NSLOT) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
 
   for (;;) {
+    /* a local batch reads the window base with its entries' loads and
+     * publishes it before the scan's barriers (thread 0) */
+    unsigned long long lctrl = 0ull;
+    unsigned lshift = 0u;
     if (S.loc_k == 0u) { /* uniform: read after a barrier */
       if (tid < 32) acquire<BLOCK>(P, S, deadline);
     } else if (tid == 0) {
-      /* next batch = the entries this CTA kept from its own last flush */
+      /* next batch = the entries this CTA kept from its own last flush
+       * (of the query whose descriptor is cached) */
       S.status = ST_LOCAL;
       S.k = S.loc_k;
       S.slot = S.loc_slot;
-      const QueryCtl *ctl = P.qs[S.q].ctl;
-      const unsigned long long c2 = ld_rlx64(&ctl->ctrl);
-      S.base_b = (unsigned)c2 & 0x7FFFFFFFu;
-      S.base_key = (unsigned)(c2 >> 32);
-      S.shift = ld_rlx32(&ctl->shift);
+      const QueryCtl *ctl = S.qd.ctl;
+      lctrl = ld_rlx64(&ctl->ctrl);
+      lshift = ld_rlx32(&ctl->shift);
+    }
+    if (tid == 0 && S.status != ST_IDLE && S.status != ST_EXIT && S.q != S.qd_q) {
+      S.qd = P.qs[S.q];
+      S.qd_q = S.q;
     }
     __syncthreads();
     const unsigned status = S.status;
@@ -688,14 +761,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
       }
     }
     const unsigned q = S.q;
-    const QueryDesc &d = P.qs[q];
+    const QueryDesc &d = S.qd;
     const unsigned *__restrict__ row = d.row;
     const uint2 *__restrict__ edges = d.edges;
     const unsigned *__restrict__ split = d.split;
     unsigned *dist = d.dist;
     const float scale = d.scale;
-    const unsigned shift = S.shift, base_b = S.base_b, base_key = S.base_key;
     unsigned k = 1;
+    unsigned cons0 = 0u, cons1 = 0u; /* page counts before this batch (thread 0) */
 
     if (status != ST_HUB) {
       k = S.k;
@@ -726,13 +799,16 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
           dp = (unsigned)(e >> 32);
         }
         if (ok) {
+          /* the row bounds are read with the distance, before the stale
+           * check: one memory round trip per batch instead of two (a wave
+           * front advances one batch per round trip chain) */
           const unsigned dv = __ldcg(dist + v);
+          const unsigned r0 = __ldg(row + v), r1 = __ldg(row + v + 1);
+          const unsigned nl = split ? __ldg(split + v) : (r1 - r0);
           ++st_items;
           if (dv < dp) {
             ++st_stale; /* superseded: a later push carries the smaller value */
           } else {
-            const unsigned r0 = __ldg(row + v), r1 = __ldg(row + v + 1);
-            const unsigned nl = split ? __ldg(split + v) : (r1 - r0);
             if (status == ST_HEAVY) { /* settled vertex: its heavy edges */
               rb = r0 + nl;
               deg = r1 - rb;
@@ -754,15 +830,22 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
       }
       S.it_rb[tid] = rb;
       S.it_du[tid] = dp;
+      if (tid == 0 && status == ST_LOCAL) {
+        S.base_b = (unsigned)lctrl & 0x7FFFFFFFu;
+        S.base_key = (unsigned)(lctrl >> 32);
+        S.shift = lshift;
+      }
       unsigned tot;
       const unsigned off = block_exscan<BLOCK>(S, chunks ? 0u : deg, tot);
       S.it_off[tid] = off;
-      /* retire the claimed range: pages whose entries are all consumed go back */
+      /* retire the claimed range (every entry has been read): the counts are
+       * raised now, and pages whose entries are all consumed go back after
+       * the expansion, when the counts have long arrived */
       if (tid == 0) {
         if (status != ST_LOCAL) {
           const unsigned c0 = min((unsigned)(ADDS_PAGE - (h & PAGE_MASK)), k);
-          consume(P, S.pi0, c0);
-          if (k > c0) consume(P, S.pi1, k - c0);
+          cons0 = consume_begin(P, S.pi0, c0);
+          if (k > c0) cons1 = consume_begin(P, S.pi1, k - c0);
         } else {
           ++st_local;
         }
@@ -819,6 +902,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
       ++st_batches;
       S.hub_chunks = 0;
     }
+    /* read after the barriers above (a local batch's base was published
+     * before the scan) */
+    const unsigned shift = S.shift, base_b = S.base_b, base_key = S.base_key;
     CY_LAP(cy_load);
 
     /* edge-balanced expansion of the batch: relax + atomicMin + stage push */
@@ -844,16 +930,20 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
                       : du + ed.y;
         }
       }
+      /* an improvement on the gathered value is applied with a reduction (no
+       * result, so no wait) and pushed at once; where a concurrent smaller
+       * value wins, the entry is dropped as stale when it is popped.  The
+       * reference's int kernel also pushes whatever its atomicMin returned
+       * (ads_int/kernel.cu:78-82). */
+      unsigned cur[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        if (nd[u] != 0xFFFFFFFFu) {
-          const unsigned cur = __ldcg(dist + dst[u]);
-          if (nd[u] < cur) {
-            const unsigned old = atomicMin(dist + dst[u], nd[u]);
-            if (old > nd[u])
-              stage<BLOCK>(S, dst[u], nd[u],
-                           bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
-          }
+        if (nd[u] < cur[u]) {
+          red_min(dist + dst[u], nd[u]);
+          stage<BLOCK>(S, dst[u], nd[u],
+                       bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
         }
       }
       __syncthreads();
@@ -864,16 +954,17 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
         ++st_mflush;
       }
     }
-    __syncthreads();
-    CY_LAP(cy_edge);
-    flush<BLOCK>(P, S, d, deadline, st_pushes, P.local_max != 0u);
-    /* batch finished: its k entries (or one chunk) leave the live count */
-    if (tid == 0) {
-      if (status != ST_HUB)
-        atomicAdd(&d.slots[S.slot].inflight, (unsigned long long)(0ull - k));
-      atomicSub(&d.ctl->live, k);
+    if (tid == 0 && (status == ST_WORK || status == ST_HEAVY)) {
+      const unsigned c0 = min((unsigned)(ADDS_PAGE - (S.h & PAGE_MASK)), k);
+      consume_end(P, S.pi0, c0, cons0);
+      if (k > c0) consume_end(P, S.pi1, k - c0, cons1);
     }
     __syncthreads();
+    CY_LAP(cy_edge);
+    /* batch finished: its k entries (or one chunk) leave the live count and
+     * the slot's in-flight count inside the flush */
+    flush<BLOCK>(P, S, d, deadline, st_pushes, P.local_max != 0u, k,
+                 status != ST_HUB ? S.slot : NO_SLOT);
     CY_LAP(cy_flush);
   }
 #undef CY_LAP
@@ -1015,7 +1106,9 @@ static cudaError_t launch_one(const EngParams &P, cudaStream_t st) {
 
 }  // namespace adds
 
-/* C++ linkage entry points used by api.cu.  block: 128, 256 or 512. */
+/* C++ linkage entry points used by api.cu.  block: 128, 256 or 512 (a
+ * 64-thread variant measured 3.6x slower on the 4096^2 grid: its CTAs hold
+ * too few of a wave front's vertices per batch). */
 cudaError_t adds_engine_prepare(bool flt, int block, int *max_blocks_per_sm) {
   switch (block) {
     case 128: return flt ? adds::prep_one<true, 128>(max_blocks_per_sm) : adds::prep_one<false, 128>(max_blocks_per_sm);

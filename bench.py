@@ -414,8 +414,11 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
             "tuned": ({k: getattr(tuned, k) for k in ("engine", "delta_shift", "block_threads",
                                                         "ctas_per_sm", "solo_max",
                                                         "hub_threshold", "light_heavy", "window",
-                                                        "batch_max", "strict_order")}
+                                                        "batch_max", "strict_order", "adapt",
+                                                        "local_max", "greed", "group_ctas",
+                                                        "dense_scan")}
                       if tuned else None),
+            "lib": os.path.relpath(A._lib.LIB_PATH, ROOT),
             "tune_ms_per_solve": tune_ms,
             "solve_kernel_ms_each": each,
             "solve_kernel_ms_median": med,
@@ -793,9 +796,14 @@ def main():
     ap.add_argument("--engine", type=int, default=0, help="0 auto, 1 async, 2 phase")
     ap.add_argument("--opts", default="", help="JSON dict of adds_opts fields to override")
     ap.add_argument("--trace", default="", help="save the phase trace of one solve (.npy)")
+    ap.add_argument("--lib", default="",
+                    help="time another build of libadds.so (A/B of two builds of the engine)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.lib:
+        import adds_b200._lib as L
+        L.LIB_PATH = os.path.abspath(args.lib)
     ws, rank, local = dist_env()
     if args.workload in ("ceiling", "comparators"):
         if rank == 0:
