@@ -8,9 +8,12 @@
  *   - several consecutive buckets may be processed at once (the reference's
  *     concur_bag, wl.h:1398-1510), the lowest is retired only once it is
  *     empty and none of its entries is still being processed (wl.h:714-724);
- *   - relax = new = d[u] + w, accept if d[v] > new, atomicMin, push
- *     (kernel.cu:112-121); float uses the IEEE bit order of non-negative
- *     floats for the 32-bit atomicMin instead of the reference's 64-bit CAS
+ *   - relax = new = d[u] + w, accept if d[v] > new, atomic minimum, push
+ *     (kernel.cu:112-121; here the minimum is a fire-and-forget reduction
+ *     and the push follows the comparison with the gathered d[v], as the
+ *     reference's int kernel pushes whatever its atomicMin returned,
+ *     kernel.cu:78-82); float uses the IEEE bit order of non-negative
+ *     floats for the 32-bit minimum instead of the reference's 64-bit CAS
  *     (ads_float/csr_graph.h:58-70); rows longer than a threshold are split
  *     across workers (wl.h:1638-1696, here across the whole grid).
  * What is new: no manager block and no CDP.  One cooperative launch of
