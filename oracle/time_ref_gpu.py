@@ -83,16 +83,23 @@ def main():
                 g.sssp_async(s, o)
             st = g.sync()
             ours_ms = st["ms"] / 8
+            # the reference's timed region leaves out its init kernel and
+            # worklist reset (ads_int/kernel.cu:225-234): the solver kernel
+            # alone is the like-for-like figure, the solve with init the
+            # conservative one
+            ours_kms = st["kernel_ms"] / 8
             res["sources"].append({
                 "src": s, "m_r": mr, "n_r": nr, "ref_ms": ref_ms, "ref_work": int(work),
                 "ref_gteps": mr / ref_ms / 1e6, "ours_ms": ours_ms, "ours_gteps": mr / ours_ms / 1e6,
-                "speedup": ref_ms / ours_ms})
+                "speedup": ref_ms / ours_ms, "ours_kernel_ms": ours_kms,
+                "speedup_kernel": ref_ms / ours_kms})
             print(json.dumps(res["sources"][-1]), flush=True)
     ok = [x for x in res["sources"] if "ref_ms" in x]
     if ok:
         res["ref_gteps_mean"] = float(np.mean([x["ref_gteps"] for x in ok]))
         res["ours_gteps_mean"] = float(np.mean([x["ours_gteps"] for x in ok]))
         res["speedup_mean"] = float(np.mean([x["speedup"] for x in ok]))
+        res["speedup_kernel_mean"] = float(np.mean([x["speedup_kernel"] for x in ok]))
     g.close()
     txt = json.dumps(res, indent=1)
     print(txt)
