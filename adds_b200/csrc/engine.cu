@@ -865,26 +865,44 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
         const unsigned u = S.loc_v[tid];
         const unsigned mask = (1u << ADDS_HUB_RING_LOG2) - 1u;
         const unsigned long long t0 = atomicAdd(&P.g->hub_tail, (unsigned long long)chunks);
-        for (unsigned c = 0; c < chunks; ++c) {
-          const unsigned long long t = t0 + c;
-          unsigned *seq = P.hub_seq + (t & mask);
-          Waiter w{deadline, 0, ADDS_DEV_HUB_OVERFLOW};
-          bool ok = true;
-          while (ld_acq32(seq) != (unsigned)t) {
-            if (!w.spin(P.g, W_HUB_PUB)) { ok = false; break; }
+        /* the row's ring cells are free once their sequence words reach
+         * their tickets: read eight at a time (one round trip each group),
+         * then one fence before all the records and one before all the
+         * sequence words, instead of two fences per chunk */
+        bool ok = true;
+        for (unsigned c0 = 0; c0 < chunks && ok; c0 += 8u) {
+          const unsigned nb = min(8u, chunks - c0);
+          unsigned sq[8];
+#pragma unroll
+          for (unsigned j = 0; j < 8u; ++j)
+            sq[j] = j < nb ? ld_rlx32(P.hub_seq + ((t0 + c0 + j) & mask)) : 0u;
+#pragma unroll
+          for (unsigned j = 0; j < 8u; ++j) {
+            if (j >= nb || !ok) continue;
+            const unsigned long long t = t0 + c0 + j;
+            Waiter w{deadline, 0, ADDS_DEV_HUB_OVERFLOW};
+            while (sq[j] != (unsigned)t) {
+              if (!w.spin(P.g, W_HUB_PUB)) { ok = false; break; }
+              sq[j] = ld_rlx32(P.hub_seq + (t & mask));
+            }
           }
-          if (!ok) break;
-          HubChunk hc;
-          hc.q = q;
-          hc.u = u;
-          hc.du = dp;
-          hc.eb = rb + c * P.hub_chunk;
-          hc.ee = (unsigned)min((unsigned long long)rb + (unsigned long long)(c + 1u) * P.hub_chunk,
-                                (unsigned long long)rb + deg);
-          hc.pad[0] = hc.pad[1] = hc.pad[2] = 0u;
-          P.hub[t & mask] = hc;
-          __threadfence();
-          st_rel32(seq, (unsigned)(t + 1ull));
+        }
+        if (ok) {
+          __threadfence(); /* the cells' last readers are done before they are reused */
+          for (unsigned c = 0; c < chunks; ++c) {
+            HubChunk hc;
+            hc.q = q;
+            hc.u = u;
+            hc.du = dp;
+            hc.eb = rb + c * P.hub_chunk;
+            hc.ee = (unsigned)min((unsigned long long)rb + (unsigned long long)(c + 1u) * P.hub_chunk,
+                                  (unsigned long long)rb + deg);
+            hc.pad[0] = hc.pad[1] = hc.pad[2] = 0u;
+            P.hub[(t0 + c) & mask] = hc;
+          }
+          __threadfence(); /* the records before their sequence words */
+          for (unsigned c = 0; c < chunks; ++c)
+            st_rlx32(P.hub_seq + ((t0 + c) & mask), (unsigned)(t0 + c + 1ull));
         }
       }
     } else { /* ST_HUB: one chunk of a split row, staged by acquire */

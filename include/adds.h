@@ -298,9 +298,9 @@ int adds_sssp_backward(adds_graph *g, uint32_t ns, const uint32_t *srcs,
  * rejected (ADDS_ERR_UNSUPPORTED); a graph within the limits whose queues
  * outgrow the fixed pool reports ADDS_ERR_WL_OVERFLOW.  The first call on a
  * device looks up the array's device address and prepares the kernels for
- * that device; make that first call before any stream capture.  All calls
- * share the array (each clears what it needs first): calls that overlap on
- * the GPU race, so issue them one after another. */
+ * that device.  All calls share the array (each clears what it needs
+ * first): calls that overlap on the GPU race, so issue them one after
+ * another. */
 #define ADDS_NOALLOC_SCRATCH_BYTES (64u << 20)
 #define ADDS_NOALLOC_MAX_N (1u << 20)
 #define ADDS_NOALLOC_MAX_M (1u << 24)
