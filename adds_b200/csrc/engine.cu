@@ -951,20 +951,33 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
                       : du + ed.y;
         }
       }
-      /* an improvement on the gathered value is applied with a reduction (no
-       * result, so no wait) and pushed at once; where a concurrent smaller
-       * value wins, the entry is dropped as stale when it is popped.  The
-       * reference's int kernel also pushes whatever its atomicMin returned
-       * (ads_int/kernel.cu:78-82). */
+      /* A single solve is a chain of dependent round trips: an improvement on
+       * the gathered value is applied with a reduction (no result, so no
+       * wait) and pushed at once; where a concurrent smaller value wins, the
+       * entry is dropped as stale when it is popped (the reference's int
+       * kernel also pushes whatever its atomicMin returned,
+       * ads_int/kernel.cu:78-82).  A batch of queries hides that latency
+       * behind its other queries and is bound by work instead: it pushes only
+       * when its atomicMin won, which spares the duplicate entries (23 % more
+       * pops on the batch of 128 grids). */
       unsigned cur[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) cur[u] = (nd[u] != 0xFFFFFFFFu) ? __ldcg(dist + dst[u]) : 0u;
+      if (P.nq == 1u) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (nd[u] < cur[u]) {
-          red_min(dist + dst[u], nd[u]);
-          stage<BLOCK>(S, dst[u], nd[u],
-                       bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
+        for (int u = 0; u < U; ++u) {
+          if (nd[u] < cur[u]) {
+            red_min(dist + dst[u], nd[u]);
+            stage<BLOCK>(S, dst[u], nd[u],
+                         bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
+          }
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (nd[u] < cur[u] && atomicMin(dist + dst[u], nd[u]) > nd[u])
+            stage<BLOCK>(S, dst[u], nd[u],
+                         bucket_slot(dist_key<FLT>(nd[u], scale), shift, base_b, base_key));
         }
       }
       __syncthreads();

@@ -241,7 +241,12 @@ int adds_graph_reached(adds_graph *g, uint64_t *reached, uint64_t *reached_edges
 /* nq solves (graph graphs[i], source srcs[i]) run in ONE persistent launch
  * with per-query bucket queues sharing one page pool; the launch is captured
  * in a CUDA graph on first run and replayed afterwards.  No reference
- * counterpart (the reference runs one source per process). */
+ * counterpart (the reference runs one source per process).  Each query
+ * takes its graph's tuned bucket width (else the heuristic).  The
+ * launch-wide knobs are opts' or the defaults, not a graph's tuned ones
+ * (those are for a plain solve that has the whole GPU).  With opts->engine
+ * 0 the engine follows the largest query's graph: asynchronous for an
+ * average degree under 6 (grids, road networks), phase otherwise. */
 int adds_batch_create(adds_graph *const *graphs, const uint32_t *srcs,
                       uint32_t nq, const adds_opts *opts, adds_batch **out);
 int adds_batch_run(adds_batch *b, adds_stats *stats);
