@@ -60,10 +60,9 @@ struct __align__(128) QueryCtl {
   unsigned long long ctrl;
   unsigned live;           /* entries pushed (queue or hub ring) not finished   */
   unsigned done;           /* 1 once live reached 0                            */
-  unsigned shift;          /* current bucket shift (device-adapted)            */
-  unsigned adapt_state;
-  unsigned long long pushes_at_base; /* controller bookkeeping                 */
-  unsigned pad[24];
+  unsigned shift;          /* bucket shift of the query                        */
+  unsigned win;            /* buckets processed at once (on-device adapted)     */
+  unsigned pad[26];
 };
 
 /* Read-only per-query descriptor. */

@@ -1010,8 +1010,11 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   k->light_heavy = o->light_heavy >= 0 ? o->light_heavy
                                        : (t->light_heavy >= 0 ? t->light_heavy
                                                               : (k->engine == ADDS_ENGINE_PHASE ? 2 : 1));
-  /* on-device bucket widening (phase engine): off unless asked or tuned */
-  k->adapt = o->adapt >= 0 ? o->adapt : (t->adapt >= 0 ? t->adapt : 0);
+  /* on-device bucket width: on in the asynchronous engine (its window on
+   * the 4096^2 grid: 20.8-23.5 ms from bucket shift 17 to 19 against
+   * 21.6-44.4 ms fixed), off in the phase engine unless asked or tuned */
+  k->adapt = o->adapt >= 0 ? o->adapt
+                           : (t->adapt >= 0 ? t->adapt : (k->engine == ADDS_ENGINE_ASYNC ? 1 : 0));
   const int hub_def = k->engine == ADDS_ENGINE_PHASE ? 256 : 16384;
   k->hub_threshold = o->hub_threshold > 0 ? o->hub_threshold : (t->hub_threshold > 0 ? t->hub_threshold : hub_def);
   k->hub_chunk = 4096;
@@ -2088,6 +2091,7 @@ extern "C" int adds_tune(adds_graph *g, const uint32_t *srcs, uint32_t ns, adds_
       try_field(&adds_opts::strict_order, {0, 1});
       try_field(&adds_opts::local_max, {0, 64, 256, 512});
       try_field(&adds_opts::light_heavy, {0, 1});
+      try_field(&adds_opts::adapt, {0, 1});
     }
     if (cur.delta_shift != s0) { /* second look around the new delta */
       std::vector<int> s2;

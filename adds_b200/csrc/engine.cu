@@ -273,6 +273,7 @@ struct Smem {
   unsigned cur_q, idle, hungry;
   unsigned loc_k, loc_slot, keep_slot;
   unsigned hub_u, ptc_q, done_late;
+  unsigned win; /* the batch's window of buckets (adapted on the device) */
   /* descriptor of query qd_q, copied once per change of query, so that a
    * batch reads its pointers from shared memory instead of HBM */
   QueryDesc qd;
@@ -328,6 +329,7 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
    * is a chain of memory round trips, each one on a wave front's path */
   const unsigned err0 = ld_rlx32(&g->err);
   const unsigned rem0 = ld_rlx32(&g->remaining);
+  const unsigned hungry0 = P.adapt ? ld_rlx32(&g->hungry) : 0u;
   unsigned long long hh0 = 0ull, ht0 = 0ull;
   if (lane == 0) {
     hh0 = ld_rlx64(&g->hub_head);
@@ -396,6 +398,7 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
     const unsigned qdone = ld_rlx32(&ctl->done);
     const unsigned long long ctrl = ld_rlx64(&ctl->ctrl);
     const unsigned qshift = ld_rlx32(&ctl->shift);
+    const unsigned qwin = ld_rlx32(&ctl->win);
     if (qdone != 0u) continue;
     const unsigned base_b = (unsigned)ctrl & 0x7FFFFFFFu;
     const bool phase_h = ((unsigned)ctrl & ADDS_PHASE_H) != 0u;
@@ -452,10 +455,21 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
         nc = ((unsigned long long)base_key << 32) | base_b | ADDS_PHASE_H;
       }
     }
+    /* On-device bucket width (adapt, the reference's dynamic delta,
+     * wl.h:968-1360): the window of buckets processed at once widens by one
+     * when this CTA finds nothing to claim inside it but light entries
+     * beyond it (the buckets run thin), and narrows by one, down to the
+     * configured window, when the base bucket retires while no CTA is idle.
+     * Any window is label-correcting, so the distances do not change. */
+    unsigned win = P.window;
+    if (P.adapt) {
+      win = qwin;
+      if (nc != ctrl && eff != 0u && hungry0 == 0u && win > P.window && lane == 0)
+        atomicCAS(&ctl->win, win, win - 1u);
+    }
     if (nc != ctrl && lane == 0) atomicCAS(&ctl->ctrl, ctrl, nc);
     /* claim: heavy list of a base in phase H (or stale lists outside the
      * window), else the lowest light bucket inside the window */
-    const unsigned win = P.window;
     const unsigned wmask_l = (eff + win >= 32u) ? (0xFFFFFFFFu << eff)
                                                 : (((1u << win) - 1u) << eff);
     /* heavy lists outside the active window belong to settled buckets */
@@ -464,7 +478,11 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
     const unsigned lcand = lamask & wmask_l;
     bool heavy = hcand != 0u;
     const unsigned j = heavy ? (__ffs(hcand) - 1u) : (lcand ? __ffs(lcand) - 1u : 32u);
-    if (j == 32u) continue;
+    if (j == 32u) {
+      if (P.adapt && win < 32u && (lamask & ~wmask_l & ~((1u << eff) - 1u)) != 0u && lane == 0)
+        atomicCAS(&ctl->win, win, win + 1u);
+      continue;
+    }
     unsigned got = 0;
     unsigned long long h0 = 0;
     if (lane == j) got = claim(heavy ? hsc : lsc, heavy ? hav : lav, P, &h0);
@@ -492,6 +510,7 @@ __device__ void acquire(const EngParams &P, Smem<BLOCK> &S,
       S.base_b = (base_b + eff) & 0x7FFFFFFFu;
       S.base_key = base_key + eff;
       S.shift = qshift;
+      S.win = win;
       S.cur_q = q;
     }
     return;
@@ -557,7 +576,7 @@ __device__ void flush(const EngParams &P, Smem<BLOCK> &S, const QueryDesc &d,
       const unsigned sh = S.base_b & 31u; /* bit r of rot = slot base_b + r */
       const unsigned rot = sh ? ((nz >> sh) | (nz << (32u - sh))) : nz;
       const unsigned r = __ffs(rot) - 1u;
-      if (r < P.window) {
+      if (r < S.win) {
         ks = (S.base_b + r) & (ADDS_NB - 1u);
         const unsigned lmax = hungry ? P.local_max_hungry : P.local_max;
         kn = min(min(__shfl_sync(0xFFFFFFFFu, c, ks), lmax), (unsigned)BLOCK);
@@ -713,6 +732,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
     S.q = S.cur_q;
     S.ptc_q = 0xFFFFFFFFu;
     S.qd_q = 0xFFFFFFFFu;
+    S.win = P.window;
   }
   if (tid < NSLOT) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
@@ -721,7 +741,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
     /* a local batch reads the window base with its entries' loads and
      * publishes it before the scan's barriers (thread 0) */
     unsigned long long lctrl = 0ull;
-    unsigned lshift = 0u;
+    unsigned lshift = 0u, lwin = 0u;
     if (S.loc_k == 0u) { /* uniform: read after a barrier */
       if (tid < 32) acquire<BLOCK>(P, S, deadline);
     } else if (tid == 0) {
@@ -733,6 +753,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
       const QueryCtl *ctl = S.qd.ctl;
       lctrl = ld_rlx64(&ctl->ctrl);
       lshift = ld_rlx32(&ctl->shift);
+      lwin = ld_rlx32(&ctl->win);
     }
     if (tid == 0 && S.status != ST_IDLE && S.status != ST_EXIT && S.q != S.qd_q) {
       S.qd = P.qs[S.q];
@@ -837,6 +858,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) solve_kernel(EngParams P)
         S.base_b = (unsigned)lctrl & 0x7FFFFFFFu;
         S.base_key = (unsigned)(lctrl >> 32);
         S.shift = lshift;
+        S.win = P.adapt ? lwin : P.window;
       }
       unsigned tot;
       const unsigned off = block_exscan<BLOCK>(S, chunks ? 0u : deg, tot);
@@ -1061,8 +1083,7 @@ __global__ void init_kernel(EngParams P) {
     c->ctrl = 0ull;
     c->done = 0u;
     c->shift = d.shift0;
-    c->adapt_state = 0u;
-    c->pushes_at_base = 0ull;
+    c->win = P.window;
     for (int s = 0; s < NSLOT; ++s) d.slots[s].inflight = 0ull;
     c->live = 1u;
     __threadfence();

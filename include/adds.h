@@ -66,10 +66,15 @@ typedef struct adds_opts {
   int32_t batch_max;     /* max vertices one CTA pops per batch; 0 = auto        */
   int32_t hub_threshold; /* out-degree above which a row is split across CTAs   */
   int32_t timeout_ms;    /* bound on every device wait; 0 = 20000 ms             */
-  int32_t adapt;         /* on-device bucket widening (phase engine): the leader
+  int32_t adapt;         /* on-device bucket widening.  Phase engine: the leader
                             merges up to 4 thin consecutive bucket slots into
-                            one light phase; -1 auto (off unless tuned), 0 off,
-                            1 on; the asynchronous engine ignores it          */
+                            one light phase.  Async engine: the window of
+                            buckets processed at once grows by one while CTAs
+                            find nothing inside it but entries beyond it, and
+                            shrinks back towards `window` as the base bucket
+                            retires with no CTA idle.  -1 auto (the tuned
+                            value, else on in the async engine and off in
+                            the phase engine), 0 off, 1 on                  */
   int32_t strict_order;  /* 1: advance a bucket only when its work is done       */
   int32_t local_max;     /* own pushes a CTA keeps as its next batch; <0 = auto,
                             0 = always go through the HBM queues              */

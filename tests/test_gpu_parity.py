@@ -352,6 +352,20 @@ def test_schedules_float_grid(window, lh, block):
                light_heavy=lh, block_threads=block)
 
 
+@pytest.mark.parametrize("window", [1, 2, 4])
+def test_async_window_adapted_on_device(window):
+    """The async engine's on-device window (adapt 1: wider while CTAs find
+    nothing inside it but entries beyond, narrower as buckets retire with no
+    CTA idle) changes the schedule, not the distances."""
+    g = G.grid(128, 96, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0, seed=31)
+    for shift in (12, 16, 20):
+        _check(g, 48 * 128 + 64, engine=ASYNC, adapt=1, window=window, delta_shift=shift)
+    r = G.rmat(13, 16, seed=32, w_hi=10000)
+    for shift in (5, 9, 12):
+        _check(r, G.max_degree_vertex(r), engine=ASYNC, adapt=1, window=window,
+               delta_shift=shift, hub_threshold=256)
+
+
 def test_non_strict_order():
     g = G.rmat(12, 16, seed=6, w_hi=10000)
     for lh in (0, 1):
