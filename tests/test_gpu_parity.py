@@ -398,6 +398,33 @@ def test_batch_mixed_graphs_replayed_twice(engine, group):
         g.close()
 
 
+@pytest.mark.parametrize("forced", [0, ASYNC, PHASE])
+def test_batch_engine_follows_average_degree(forced):
+    """With the engine left on auto, a batch of grids (average degree about
+    4) runs on the asynchronous engine and a batch of R-MAT graphs (16) on
+    the phase engine; a named engine wins.  A graph's single-solve tuning
+    does not decide it.  Distances equal the oracle's either way."""
+    grids = [G.grid(64 + 16 * i, 40 + 8 * i, 0.02, 8, wtype=G.F32, w_lo=1.0, w_hi=100.0,
+                    seed=60 + i) for i in range(3)]
+    rmats = [G.rmat(11 + (i % 2), 16, seed=70 + i, w_hi=5000) for i in range(3)]
+    for csrs, auto in ((grids, ASYNC), (rmats, PHASE)):
+        graphs = [A.Graph.from_csr(c) for c in csrs]
+        try:
+            if csrs is rmats:  # tuned for plain solves: must not steer the batch
+                graphs[-1].tune([1], A.default_opts(engine=ASYNC))
+            srcs = [3, 7, 11]
+            b = A.Batch(graphs, srcs, A.default_opts(**OPTS, engine=forced))
+            st = b.run()
+            assert st["engine"] == (forced or auto)
+            for q, (c, s) in enumerate(zip(csrs, srcs)):
+                ref, _ = O.dijkstra(c, s)
+                assert np.array_equal(b.dist(q), ref), f"query {q}"
+            b.close()
+        finally:
+            for g in graphs:
+                g.close()
+
+
 def test_cli_int_matches_reference_text(tmp_path):
     import os
     import subprocess
