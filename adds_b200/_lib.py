@@ -60,7 +60,8 @@ class Opts(C.Structure):
         ("solo_max", C.c_int32),
         ("near_far", C.c_int32),
         ("dense_scan", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("pull", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

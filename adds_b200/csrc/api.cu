@@ -268,6 +268,7 @@ struct Knobs {
   int window, ctas_per_sm, batch_max, hub_threshold, hub_chunk, strict, adapt, local_max,
       light_heavy, block, greed;
   int engine, variant, group_ctas, solo_max, near_far, dense_scan; /* phase engine */
+  int pull; /* phase engine: heavy phases may run as a pull (in-edge CSR)     */
   unsigned long long timeout_ns;
 };
 
@@ -394,6 +395,9 @@ struct adds_graph {
   unsigned *split = nullptr;   /* light-edge count per row for split_thr      */
   unsigned split_thr = 0;
   bool sorted_valid = false, split_valid = false;
+  unsigned *trow = nullptr;    /* in-edge CSR (pull phases): n+1 offsets      */
+  uint2 *tedges = nullptr;     /* {tail vertex, weight bits} per in-edge      */
+  bool trans_valid = false;
   unsigned long long wversion = 0; /* bumped by adds_graph_set_weights */
   unsigned *aux = nullptr;        /* 64 B: validation flag + weight sample sum */
   uint32_t *sort_buf = nullptr;   /* 4*m words: keys/values in and out          */
@@ -564,6 +568,8 @@ extern "C" void adds_graph_free(adds_graph *g) {
   if (g->dist) cudaFree(g->dist);
   if (g->sedges) cudaFree(g->sedges);
   if (g->split) cudaFree(g->split);
+  if (g->trow) cudaFree(g->trow);
+  if (g->tedges) cudaFree(g->tedges);
   if (g->aux) cudaFree(g->aux);
   if (g->sort_buf) cudaFree(g->sort_buf);
   if (g->sort_tmp) cudaFree(g->sort_tmp);
@@ -939,6 +945,7 @@ extern "C" int adds_graph_set_weights(adds_graph *g, const void *w) {
   memcpy(&sw, h + 2, 8);
   g->avg_w = sw / ns;
   g->sorted_valid = g->split_valid = false; /* the weight order changed */
+  g->trans_valid = false;                   /* the in-edges carry weights */
   ++g->wversion;
   return ADDS_OK;
 }
@@ -1030,6 +1037,10 @@ static void resolve(const adds_graph *g, const adds_opts *o, Knobs *k, int *shif
   /* dense bucket slots: explicit > tuned > off (measured on R-MAT 24: the
    * scans remove the stale entries but cost as much as they save) */
   k->dense_scan = o->dense_scan != 0 ? o->dense_scan : (t->dense_scan != 0 ? t->dense_scan : -1);
+  /* pull heavy phases: 1 asked for, 0 off, 2 automatic (graphs of at least
+   * 2^22 edges; the leader still picks push wherever the counted pull would
+   * read more edges) */
+  k->pull = o->pull != 0 ? (o->pull > 0 ? 1 : 0) : (t->pull != 0 ? (t->pull > 0 ? 1 : 0) : 2);
   const int tmo = o->timeout_ms > 0 ? o->timeout_ms : 20000;
   k->timeout_ns = (unsigned long long)tmo * 1000000ull;
 }
@@ -1156,6 +1167,90 @@ static int graph_layout(adds_graph *g, const Knobs &k, int shift, float scale,
   return ADDS_OK;
 }
 
+/* In-edge CSR for pull phases: in-degrees by atomic counts, their exclusive
+ * scan, then each out-edge u -> v written as {u, w} at a cursor of v (the
+ * order inside an in-row is whatever the atomics give; a pull takes the
+ * minimum over the row, which does not depend on it).  A warp per tail
+ * vertex reads its row coalesced. */
+__global__ void k_indeg(const uint2 *e, uint64_t m, unsigned *cnt) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + e[i].x, 1u);
+}
+__global__ void k_transpose(const unsigned *row, const uint2 *e, uint32_t n, unsigned *cur,
+                            uint2 *te) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t wstride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; u < n; u += wstride) {
+    const unsigned r1 = row[u + 1];
+    for (unsigned i = row[u] + lane; i < r1; i += 32u) {
+      const uint2 x = e[i];
+      te[atomicAdd(cur + x.x, 1u)] = make_uint2((unsigned)u, x.y);
+    }
+  }
+}
+
+static int graph_transposed(adds_graph *g) {
+  if (g->trans_valid) return ADDS_OK;
+  const size_t n = g->n, m = g->m;
+  if (!g->trow || !g->tedges) {
+    if (g->trow) cudaFree(g->trow);
+    g->trow = nullptr;
+    CK(cudaMalloc(&g->trow, (n + 1) * 4));
+    const cudaError_t ea = cudaMalloc(&g->tedges, (m + ADDS_EDGE_PAD) * sizeof(uint2));
+    if (ea != cudaSuccess) {
+      cudaFree(g->trow);
+      g->trow = nullptr;
+      g->tedges = nullptr;
+      return cuda_fail(ea, "transposed graph");
+    }
+    CK(cudaMemsetAsync(g->tedges + m, 0, ADDS_EDGE_PAD * sizeof(uint2), g->stream));
+    g->bytes += (n + 1) * 4 + m * sizeof(uint2);
+  }
+  unsigned *cnt = nullptr;
+  void *tmp = nullptr;
+  size_t tb = 0;
+  int rc = ADDS_OK;
+  cudaError_t e = cudaMalloc(&cnt, (n + 1) * 4);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, (n + 1) * 4, g->stream);
+  if (e == cudaSuccess && m) {
+    k_indeg<<<4 * 148, 256, 0, g->stream>>>(g->edges, m, cnt);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, g->trow, (int)(n + 1), g->stream);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, tb ? tb : 16);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, g->trow, (int)(n + 1), g->stream);
+  /* the cursors start at the row offsets */
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, g->trow, n * 4, cudaMemcpyDeviceToDevice, g->stream);
+  if (e == cudaSuccess && m) {
+    k_transpose<<<4 * 148, 256, 0, g->stream>>>(g->row, g->edges, g->n, cnt, g->tedges);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) rc = cuda_fail(e, "transposed graph");
+  if (cnt) cudaFree(cnt);
+  if (tmp) cudaFree(tmp);
+  if (!rc) g->trans_valid = true;
+  return rc;
+}
+
+/* The in-edge CSR of q's graph when pull phases may run on it (phase engine,
+ * light/heavy split, bucket ring; automatic: 2^22 edges or more, where a
+ * heavy phase is long enough to pay for the extra launches of a pull); else
+ * none. */
+static int phase_pull_arrays(adds_graph *g, const Knobs &k, PhQuery *q) {
+  q->trow = nullptr;
+  q->tedges = nullptr;
+  if (!k.pull || !q->split || k.near_far || g->m == 0) return ADDS_OK;
+  if (k.pull == 2 && g->m < (1ull << 22)) return ADDS_OK;
+  if (g->n >= 0x7FFFFFFFu || g->m >= 0xFFFFFFFFull) return ADDS_OK; /* 32-bit offsets */
+  const int rc = graph_transposed(g);
+  if (rc) return rc;
+  q->trow = g->trow;
+  q->tedges = g->tedges;
+  return ADDS_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* plain solves                                                               */
 static int graph_engine(adds_graph *g, const Knobs &k, int shift, float scale) {
@@ -1197,11 +1292,14 @@ static int graph_phase_engine(adds_graph *g, const Knobs &k, int shift, float sc
   q.scale = scale;
   q.shift = (unsigned)shift;
   q.m = g->m;
+  rc = phase_pull_arrays(g, k, &q);
+  if (rc) return rc;
   PhEngine &E = g->peng;
   if (E.nq == 1 && E.variant == (unsigned)k.variant && E.req_group == k.group_ctas &&
       ph_hub_chunk(phase_knobs(k)) >= E.hub_eff) {
     PhQuery &h = E.qs_host[0];
-    if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale)
+    if (h.edges == edges && h.split == split && h.shift == q.shift && h.scale == scale &&
+        h.trow == q.trow)
       return ADDS_OK;
     E.qs_host[0] = q;
     return ph_engine_upload(E, g->stream) ? ADDS_ERR_CUDA : ADDS_OK;
@@ -1614,6 +1712,12 @@ static int batch_phase_engine(adds_batch *b) {
     q.scale = b->scales[i];
     q.shift = (unsigned)b->shifts[i];
     q.m = g->m;
+    /* a pull phase ends a launch, which the groups of a batch do not share:
+     * only a batch of one query pulls */
+    if (qv.size() == 1) {
+      const int rp = phase_pull_arrays(g, b->kn, &q);
+      if (rp) return rp;
+    }
     qv[i] = q;
   }
   if (b->exec) {
@@ -1793,8 +1897,13 @@ static int batch_relayout(adds_batch *b) {
     const int rc = graph_layout(b->qgraph[i], b->kn, b->shifts[i], b->scales[i], &edges, &split);
     if (rc) return rc;
     if (b->kn.engine == ADDS_ENGINE_PHASE) {
-      b->peng.qs_host[i].edges = edges;
-      b->peng.qs_host[i].split = split;
+      PhQuery &q = b->peng.qs_host[i];
+      q.edges = edges;
+      q.split = split;
+      if (b->qgraph.size() == 1) { /* new weights for the in-edge copy */
+        const int rp = phase_pull_arrays(b->qgraph[i], b->kn, &q);
+        if (rp) return rp;
+      }
     } else {
       b->eng.qs_host[i].edges = edges;
       b->eng.qs_host[i].split = split;

@@ -108,6 +108,25 @@ __device__ __forceinline__ unsigned bucket_of(unsigned d, float scale, unsigned 
   if (FLT) key = __float2uint_rz(__fmul_rn(__uint_as_float(d), scale));
   return key >> shift;
 }
+/* A lower bound of every heavy-edge candidate fl(d[u] + w) out of bucket
+ * base: a vertex whose distance is at or below it cannot be improved by the
+ * bucket's heavy edges.  Integer keys: a heavy edge has w >= 2^shift and d[u]
+ * >= base << shift, so the bound is the next bucket's first key (minus one).
+ * Float keys: d[u] >= base 2^shift / scale and w >= 2^shift / scale up to the
+ * roundings of the key product and of the light threshold, both covered by
+ * the 1e-6 margin; the sum is rounded down. */
+template <bool FLT>
+__device__ __forceinline__ unsigned pull_floor(const PhQuery &Q, unsigned base) {
+  if (!FLT) {
+    const unsigned long long t = ((unsigned long long)base + 1ull) << Q.shift;
+    return t > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)(t - 1ull);
+  }
+  const double bw = ldexp(1.0, (int)Q.shift) / (double)Q.scale * (1.0 - 1e-6);
+  const float lo = __double2float_rd((double)base * bw);
+  const float dw = __double2float_rd(bw);
+  return __float_as_uint(__fadd_rd(lo, dw));
+}
+
 /* list of a push with bucket b relative to the base bucket being settled;
  * the near-far schedule keeps one far pile instead of the ring */
 __device__ __forceinline__ unsigned route(unsigned b, unsigned base, unsigned near_far) {
@@ -121,6 +140,7 @@ __device__ __forceinline__ unsigned route(unsigned b, unsigned base, unsigned ne
 /* shared memory of one CTA                                                   */
 #define PH_RES_PAGES 6u /* pages one list reservation may touch (flush size) */
 #define PH_EPT 1        /* frontier entries one thread prepares per chunk     */
+#define PH_PULL_V 4u    /* vertices one thread selects per pull tile          */
 /* split-row chunk records one CTA takes at a time */
 #define PH_HUB_PER_CLAIM(BLOCK) ((BLOCK) / 16u)
 
@@ -140,6 +160,8 @@ struct PSmem {
   unsigned it_rb[IC];
   unsigned it_du[IC];      /* distance the item is expanded with                 */
   unsigned it_off[IC + 1]; /* exclusive scan of the segment lengths              */
+  unsigned it_d0[IC];      /* pull batch: each vertex's distance before it       */
+  unsigned it_v[IC];       /* pull batch: the item's vertex                      */
   unsigned ck_k, ck_E;        /* items and edges of the chunk                    */
   unsigned pb_v[SB];
   unsigned pb_d[SB];
@@ -159,9 +181,26 @@ struct PSmem {
                                waits), expand, flush, barrier wait, leader,
                                grid-phase work, total */
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
+  /* pull phase: next tile of the current run, tiles left in it, the tile
+   * being expanded, pull_floor of the phase's bucket */
+  unsigned pl_t0, pl_k, pl_cur, pl_T;
+  /* thread 0's claim state and cycle marks (kept here, not in registers) */
+  unsigned long long local_claim, pend;
+  long long tph, tk, cy0;
+  unsigned long long nphase;
   unsigned hub_made; /* this CTA cut a row into records in the current phase */
   unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
 };
+
+/* thread 0's cycle accounting: the cycles since the last mark go to cy[i] */
+template <int BLOCK, int UU>
+__device__ __forceinline__ void cy_mark(PSmem<BLOCK, UU> &S, int i) {
+  if (threadIdx.x == 0) {
+    const long long t = clock64();
+    S.cy[i] += (unsigned long long)(t - S.tph);
+    S.tph = t;
+  }
+}
 
 /* what a CTA keeps for the kernel's lifetime; the group's arrays are
  * recomputed from the parameters where they are used */
@@ -483,10 +522,10 @@ __device__ __forceinline__ void finish_items(PSmem<BLOCK, UU> &S, unsigned k, un
 }
 
 /* Claims and prepares the next chunk.  Returns false when the phase has no
- * more chunks.  Every thread calls it. */
+ * more chunks.  Every thread calls it; thread 0 keeps the claim state in
+ * shared memory (S.local_claim, S.pend), out of every thread's registers. */
 template <bool FLT, int BLOCK, int UU>
-__device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo,
-                              unsigned long long &local_claim, unsigned long long &pend) {
+__device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo) {
   const unsigned tid = threadIdx.x;
   const unsigned mode = S.D.mode;
   PhGroup *G = grp_of(P, c);
@@ -510,13 +549,14 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
     unsigned long long at;
     unsigned n;
     if (solo) {
-      at = local_claim;
+      at = S.local_claim;
       n = IC;
-      local_claim += IC;
+      S.local_claim = at + IC;
     } else {
       /* the next claim is taken one chunk ahead, so its latency overlaps this
        * chunk's work; claims past the end are simply not used.  pend packs
        * the claim's start (entries since work_base, 40 bits) and size. */
+      unsigned long long pend = S.pend;
       if (pend == ~0ull) {
         const unsigned w = want(0ull);
         pend = ((atomicAdd(&G->work, (unsigned long long)w) - d_wb) << 24) | w;
@@ -524,7 +564,7 @@ __device__ bool prepare_chunk(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bo
       at = pend >> 24;
       n = (unsigned)(pend & 0xFFFFFFull);
       const unsigned w = want(at + n);
-      pend = ((atomicAdd(&G->work, (unsigned long long)w) - d_wb) << 24) | w;
+      S.pend = ((atomicAdd(&G->work, (unsigned long long)w) - d_wb) << 24) | w;
     }
     S.claim = at;
     S.stop = at >= count ? 1u : 0u;
@@ -691,7 +731,9 @@ __device__ bool prepare_records(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) 
  * search from the previous one.  The loads of iteration i+1 are issued
  * before the distance gathers of iteration i.  Every SEGI iterations the CTA
  * meets once to flush staged pushes (the staging buffer is sized so that this
- * is the only barrier needed). */
+ * is the only barrier needed).  (The pull direction has a loop of its own,
+ * pull_tile_warp, in a kernel of its own: a run-time switch inside this loop
+ * cost it 37 % of its speed on R-MAT 24.) */
 template <bool FLT, int BLOCK, int UU>
 __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q,
                        unsigned base) {
@@ -778,13 +820,223 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
 }
 
 /* ------------------------------------------------------------------------ */
+/* A heavy phase run as a pull (PH_M_PULL; the leader picks it when the heavy
+ * scan counted fewer in-edges into the vertices above pull_floor than heavy
+ * edges out of the settled bucket).  Every vertex above pull_floor -- the
+ * only ones the bucket's heavy edges can improve -- takes the minimum of
+ * fl(d[u] + w) over all its in-edges; one that improves is pushed once, with
+ * that value.  The distances equal the push phase's: every candidate is the
+ * length of a path, and each heavy edge out of the bucket into such a vertex
+ * is one of its in-edges.  Only the thread that owns a vertex writes it in
+ * this phase.  The direction choice follows Beamer et al. (SC 2012), applied
+ * to delta-stepping's heavy phase as in Chakaravarthy et al. (IPDPS 2014).
+ *
+ * CTAs claim runs of tiles of PH_PULL_V x BLOCK vertices (guided
+ * self-scheduling, the next run claimed one run ahead; thread 0 keeps the
+ * runs in shared memory) and run each through pull_tile.  Claims the next
+ * tile into S.pl_cur; false when none is left.  Every thread calls it. */
+template <bool FLT, int BLOCK, int UU>
+__device__ bool prepare_pull(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q) {
+  const unsigned tid = threadIdx.x;
+  const unsigned long long tv = (unsigned long long)PH_PULL_V * BLOCK;
+  const unsigned ntile = (unsigned)(((unsigned long long)Q.n + tv - 1ull) / tv);
+  __syncthreads(); /* everyone has read the previous tile's S.pl_cur and S.stop */
+  if (tid == 0) {
+    if (S.pl_k == 0u) { /* the run claimed ahead becomes current; claim the next */
+      PhGroup *G = grp_of(P, c);
+      const unsigned long long wb = S.D.work_base;
+      /* about a quarter of this CTA's share of what is left, 1 to 8 tiles;
+       * packed (start << 24) | count */
+      auto take = [&](unsigned long long seen) {
+        const unsigned long long left = ntile > seen ? ntile - seen : 0ull;
+        const unsigned long long w = min(8ull, max(1ull, left / (4ull * P.gsize)));
+        return ((atomicAdd(&G->work, w) - wb) << 24) | w;
+      };
+      unsigned long long pend = S.pend;
+      if (pend == ~0ull) pend = take(0ull);
+      S.pl_t0 = (unsigned)min(pend >> 24, (unsigned long long)ntile);
+      S.pl_k = (unsigned)(pend & 0xFFFFFFull);
+      S.pend = take((pend >> 24) + (pend & 0xFFFFFFull));
+    }
+    S.pl_cur = S.pl_t0;
+    S.stop = S.pl_t0 >= ntile ? 1u : 0u;
+    ++S.pl_t0;
+    --S.pl_k;
+  }
+  __syncthreads();
+  return S.stop == 0u;
+}
+
+/* lane-wise inclusive scan over a warp */
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned x) {
+  const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= (unsigned)o) x += y;
+  }
+  return x;
+}
+
+/* One claimed pull tile, PH_PULL_V x BLOCK consecutive vertices, each warp
+ * on its own 32 x PH_PULL_V of them with no block barrier (the block-wide
+ * version spent 40 % of its issue slots waiting at barriers).  A lane
+ * selects its vertices above pull_floor that have in-edges; the warp
+ * compacts them into its 32-item slice of the chunk arrays, 32 at a time,
+ * spreads the slice's in-edges over its lanes (U per lane per round, the
+ * next round's edge loads issued before this round's gathers) and lowers
+ * each item's best candidate with a shared-memory atomic minimum; a vertex
+ * whose best is below its distance stores it (only this lane writes the
+ * vertex in the phase) and is staged for its bucket (a tile stages at most
+ * one push per vertex, which the staging buffer holds past FLUSH_AT).  Every
+ * thread calls it; the caller meets the block at a barrier before the flush
+ * check. */
+template <bool FLT, int BLOCK, int UU>
+__device__ void pull_tile_warp(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S,
+                               const PhQuery &Q) {
+  constexpr unsigned V = PH_PULL_V, U = PSmem<BLOCK, UU>::U, R = 32u * U;
+  constexpr unsigned SB = PSmem<BLOCK, UU>::SB, FLUSH_AT = PSmem<BLOCK, UU>::FLUSH_AT;
+  static_assert(PSmem<BLOCK, UU>::IC == BLOCK, "one 32-item slice per warp");
+  static_assert(FLUSH_AT + V * BLOCK <= SB, "a tile's pushes fit the staging buffer");
+  const unsigned tid = threadIdx.x, lane = tid & 31u, sl = tid & ~31u;
+  unsigned *const w_rb = S.it_rb + sl, *const w_best = S.it_du + sl, *const w_d0 = S.it_d0 + sl;
+  unsigned *const w_v = S.it_v + sl, *const w_off = S.it_off + sl;
+  const uint2 *__restrict__ edges = Q.tedges;
+  unsigned *const dist = Q.dist;
+  const unsigned n = Q.n, T = S.pl_T;
+  const unsigned long long v0 = ((unsigned long long)S.pl_cur * BLOCK + tid) * V;
+  unsigned d[V], rb[V], re[V];
+  const bool vec = ((reinterpret_cast<unsigned long long>(Q.dist) |
+                     reinterpret_cast<unsigned long long>(Q.trow)) & 15ull) == 0ull;
+  if (vec && v0 + V <= n) {
+    const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(Q.dist + v0));
+    const uint4 r = __ldg(reinterpret_cast<const uint4 *>(Q.trow + v0));
+    d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
+    rb[0] = r.x; rb[1] = r.y; rb[2] = r.z; rb[3] = r.w;
+    re[0] = r.y; re[1] = r.z; re[2] = r.w; re[3] = __ldg(Q.trow + v0 + 4);
+  } else {
+#pragma unroll
+    for (unsigned j = 0; j < V; ++j) {
+      const bool in = v0 + j < n;
+      d[j] = in ? __ldcg(Q.dist + v0 + j) : 0u;
+      rb[j] = in ? __ldg(Q.trow + v0 + j) : 0u;
+      re[j] = in ? __ldg(Q.trow + v0 + j + 1) : 0u;
+    }
+  }
+  unsigned selm = 0;
+#pragma unroll
+  for (unsigned j = 0; j < V; ++j)
+    if (v0 + j < n && d[j] > T && re[j] > rb[j]) selm |= 1u << j;
+  const unsigned cnt = __popc(selm), incl = warp_incl_scan(cnt);
+  const unsigned total = __shfl_sync(0xFFFFFFFFu, incl, 31), pos0 = incl - cnt;
+  if (lane == 0 && total != 0u) atomicAdd(&S.st_items, (unsigned long long)total);
+  unsigned nedges = 0;
+  for (unsigned r0 = 0; r0 < total; r0 += 32u) {
+    __syncwarp(); /* the last batch's items are read */
+    unsigned p = pos0;
+#pragma unroll
+    for (unsigned j = 0; j < V; ++j) {
+      if ((selm >> j) & 1u) {
+        if (p - r0 < 32u) { /* p in [r0, r0 + 32) */
+          const unsigned i = p - r0;
+          w_rb[i] = rb[j];
+          w_best[i] = d[j]; /* the item's best candidate so far */
+          w_d0[i] = d[j];
+          w_v[i] = (unsigned)(v0 + j);
+          w_off[i] = re[j] - rb[j]; /* the length, turned into an offset below */
+        }
+        ++p;
+      }
+    }
+    __syncwarp();
+    const unsigned k = min(32u, total - r0);
+    const unsigned len = lane < k ? w_off[lane] : 0u;
+    const unsigned li = warp_incl_scan(len);
+    const unsigned E = __shfl_sync(0xFFFFFFFFu, li, 31);
+    w_off[lane] = li - len; /* each lane rewrites the slot it read */
+    __syncwarp();
+    unsigned lo = 0; /* item of the lane's last edge: its edges only move forward */
+    uint2 ne[U];
+    unsigned nu[U];
+    auto find = [&](unsigned e) {
+      /* gallop: the last item whose offset is <= e, at or after lo */
+      unsigned step = 1u;
+      while (lo + step < k && w_off[lo + step] <= e) {
+        lo += step;
+        step <<= 1;
+      }
+      unsigned hi = min(lo + step, k) - 1u;
+      while (lo < hi) {
+        const unsigned mid = (lo + hi + 1u) >> 1;
+        if (w_off[mid] <= e) lo = mid; else hi = mid - 1u;
+      }
+    };
+    auto load_round = [&](unsigned eb) {
+#pragma unroll
+      for (unsigned u = 0; u < U; ++u) {
+        const unsigned e = eb + u * 32u + lane;
+        nu[u] = 0xFFFFFFFFu;
+        ne[u] = make_uint2(0u, 0u);
+        if (e < E) {
+          find(e);
+          ne[u] = ld_edge(edges + w_rb[lo] + (e - w_off[lo]));
+          nu[u] = lo;
+        }
+      }
+    };
+    const unsigned nit = (E + R - 1u) / R;
+    if (nit) load_round(0u);
+    for (unsigned it = 0; it < nit; ++it) {
+      unsigned src[U], cur[U], wv[U], iv[U], live = 0;
+#pragma unroll
+      for (unsigned u = 0; u < U; ++u) {
+        src[u] = ne[u].x;
+        wv[u] = ne[u].y;
+        iv[u] = nu[u];
+        if (nu[u] != 0xFFFFFFFFu) {
+          live |= 1u << u;
+          ++nedges;
+        }
+      }
+      if (it + 1u < nit) load_round((it + 1u) * R);
+#pragma unroll
+      for (unsigned u = 0; u < U; ++u) cur[u] = ((live >> u) & 1u) ? __ldcg(dist + src[u]) : 0u;
+#pragma unroll
+      for (unsigned u = 0; u < U; ++u) {
+        if ((live >> u) & 1u) {
+          /* an unreached tail gives INF + w, above every distance */
+          const unsigned w = wv[u], i = iv[u];
+          const unsigned cand =
+              FLT ? __float_as_uint(__fadd_rn(__uint_as_float(cur[u]), __uint_as_float(w)))
+                  : cur[u] + w;
+          if (cand < w_best[i]) atomicMin(&w_best[i], cand);
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < k) {
+      const unsigned best = w_best[lane];
+      if (best < w_d0[lane]) {
+        const unsigned v = w_v[lane];
+        st_rlx32(dist + v, best);
+        stage<BLOCK, UU>(S, v, best, route(bucket_of<FLT>(best, Q.scale, Q.shift), S.D.base,
+                                           P.near_far));
+      }
+    }
+  }
+  c.edges += nedges;
+}
+
+
+/* ------------------------------------------------------------------------ */
 /* One phase (or, solo, the whole of it on this CTA).                         */
 template <bool FLT, int BLOCK, int UU>
 __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo) {
   constexpr unsigned FLUSH_AT = PSmem<BLOCK, UU>::FLUSH_AT;
   const unsigned tid = threadIdx.x;
   const unsigned mode = S.D.mode;
-  if (mode == PH_M_START || mode == PH_M_EXIT) return;
+  /* a pull phase runs in its own kernel (pull_kernel) between two launches */
+  if (mode == PH_M_START || mode == PH_M_EXIT || mode == PH_M_PULL) return;
   const PhQuery &Q = P.qs[S.D.q];
   if (mode == PH_M_INIT) {
     const unsigned rank = solo ? 0u : c.rank;
@@ -811,21 +1063,30 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
      * move.  A CTA takes tiles of 4 x BLOCK vertices round-robin, SCANG of
      * them per round with all their 16-byte loads issued first; each tile's
      * matches are staged (at most 4 x BLOCK) before the flush check, which
-     * the staging buffer's size allows. */
+     * the staging buffer's size allows.  A sampling heavy scan (D.sample)
+     * stages nothing: over one tile in PH_SAMPLE_STRIDE it sums, for the
+     * leader's push-or-pull choice, the heavy out-edges of the bucket and
+     * the in-edges of the vertices above pull_floor. */
     constexpr unsigned SCANG = 4;
     const bool heavy = S.D.list == PH_LSETTLED;
+    const bool sample = heavy && S.D.sample != 0u;
+    const bool count = sample && Q.trow != nullptr;
+    const unsigned tstep = sample ? PH_SAMPLE_STRIDE : 1u;
+    const unsigned pfl = count ? pull_floor<FLT>(Q, S.D.base) : 0xFFFFFFFFu;
+    unsigned long long c_push = 0, c_pull = 0;
     const unsigned target = heavy ? PH_LSETTLED : PH_LNEXT;
     const unsigned base = S.D.base, n = Q.n;
     const unsigned inf = P.is_float ? 0x7F7FFFFFu : 0x7FFFFFFFu;
     const bool vec = (reinterpret_cast<unsigned long long>(Q.dist) & 15ull) == 0ull;
-    const unsigned ntile = (n + 4u * BLOCK - 1u) / (4u * BLOCK);
+    /* tiles read (every tstep-th tile of 4 x BLOCK vertices) */
+    const unsigned ntile = ((n + 4u * BLOCK - 1u) / (4u * BLOCK) + tstep - 1u) / tstep;
     const unsigned r0 = solo ? 0u : c.rank, stride = solo ? 1u : P.gsize;
     for (unsigned t0 = r0; t0 < ntile; t0 += SCANG * stride) {
       unsigned d[SCANG][4];
 #pragma unroll
       for (unsigned g = 0; g < SCANG; ++g) {
         const unsigned t = t0 + g * stride;
-        const unsigned v0 = t * 4u * BLOCK + 4u * tid;
+        const unsigned v0 = t * tstep * 4u * BLOCK + 4u * tid;
         if (t < ntile && vec && v0 + 3u < n) {
           const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(Q.dist + v0));
           d[g][0] = x.x;
@@ -840,38 +1101,53 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
       }
 #pragma unroll
       for (unsigned g = 0; g < SCANG; ++g) {
-        const unsigned v0 = (t0 + g * stride) * 4u * BLOCK + 4u * tid;
+        const unsigned v0 = (t0 + g * stride) * tstep * 4u * BLOCK + 4u * tid;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           bool take = d[g][j] != inf && bucket_of<FLT>(d[g][j], Q.scale, Q.shift) == base;
           if (take && heavy) {
             const unsigned v = v0 + j;
-            take = __ldg(Q.split + v) < __ldg(Q.row + v + 1) - __ldg(Q.row + v);
+            const unsigned nl = __ldg(Q.split + v), deg = __ldg(Q.row + v + 1) - __ldg(Q.row + v);
+            take = nl < deg;
+            c_push += deg - nl;
           }
-          if (take) stage<BLOCK, UU>(S, v0 + j, d[g][j], target);
+          if (take && !sample) stage<BLOCK, UU>(S, v0 + j, d[g][j], target);
+          if (count && d[g][j] > pfl && v0 + j < n)
+            c_pull += __ldg(Q.trow + v0 + j + 1) - __ldg(Q.trow + v0 + j);
         }
         __syncthreads();
         if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
       }
     }
     flush<BLOCK, UU>(P, c, S);
+    if (count) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        c_push += __shfl_down_sync(0xFFFFFFFFu, c_push, o);
+        c_pull += __shfl_down_sync(0xFFFFFFFFu, c_pull, o);
+      }
+      if ((tid & 31u) == 0u) {
+        PhGroup *G = grp_of(P, c);
+        if (c_push) atomicAdd(&G->pc_push, c_push);
+        if (c_pull) atomicAdd(&G->pc_pull, c_pull);
+      }
+    }
     return;
   }
   const unsigned base = S.D.base;
-  unsigned long long local_claim = 0, pend = ~0ull;
   /* frontier chunks first, then split-row records (a records-only phase
    * finishes what a solo phase left) */
   bool records = mode == PH_M_HUB;
-  if (tid == 0) S.hub_made = 0u; /* read after the claim barriers below */
-  long long t0 = clock64();
+  if (tid == 0) {
+    S.hub_made = 0u; /* read after the claim barriers below */
+    S.local_claim = 0ull;
+    S.pend = ~0ull;
+    S.tph = clock64();
+  }
   for (;;) {
     const bool have = records ? prepare_records<FLT, BLOCK, UU>(P, c, S)
-                              : prepare_chunk<FLT, BLOCK, UU>(P, c, S, solo, local_claim, pend);
-    {
-      const long long t1 = clock64();
-      if (tid == 0) S.cy[records ? 1 : 0] += (unsigned long long)(t1 - t0);
-      t0 = t1;
-    }
+                              : prepare_chunk<FLT, BLOCK, UU>(P, c, S, solo);
+    cy_mark<BLOCK, UU>(S, records ? 1 : 0);
     if (!have) {
       if (records) break;
 
@@ -894,20 +1170,12 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
     }
     if (S.ck_E != 0u) expand<FLT, BLOCK, UU>(P, c, S, Q, base);
     __syncthreads();
-    {
-      const long long t1 = clock64();
-      if (tid == 0) S.cy[2] += (unsigned long long)(t1 - t0);
-      t0 = t1;
-    }
+    cy_mark<BLOCK, UU>(S, 2);
     if (S.pcnt > FLUSH_AT) flush<BLOCK, UU>(P, c, S);
-    {
-      const long long t1 = clock64();
-      if (tid == 0) S.cy[3] += (unsigned long long)(t1 - t0);
-      t0 = t1;
-    }
+    cy_mark<BLOCK, UU>(S, 3);
   }
   flush<BLOCK, UU>(P, c, S);
-  if (tid == 0) S.cy[3] += (unsigned long long)(clock64() - t0);
+  cy_mark<BLOCK, UU>(S, 3);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -926,6 +1194,10 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   unsigned nx = 0, xl[PH_MAXR - 1] = {0u, 0u, 0u}, full = 0u;
   unsigned long long xlo[PH_MAXR - 1] = {0ull, 0ull, 0ull}, xhi[PH_MAXR - 1] = {0ull, 0ull, 0ull};
   bool decide = false, next_query = false;
+  /* the heavy scan that just ran counted push and pull work (read once: the
+   * flag holds for this decision only) */
+  const unsigned pcs = ld_rlx32(&G->pc_state);
+  unsigned pc_next = 0u, sample = 0u;
   if (ld_rlx32(&P.g->err) != 0u) {
     mode = PH_M_EXIT;
   } else if (prev_mode == PH_M_START) {
@@ -997,14 +1269,38 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     } else if (ts > hs) {
       /* a large settled list (duplicates included) is rebuilt once by a
        * heavy scan: each settled vertex with heavy edges once, in vertex
-       * order; the list's entries are dropped */
+       * order; the list's entries are dropped.  With an in-edge CSR the scan
+       * also counts both directions, and the bucket's heavy edges are then
+       * taken as a pull when that reads fewer edges than the push */
       const PhQuery &Qh = P.qs[q];
       const unsigned long long thr = max(4096u, Qh.n >> (P.dense_shift ? P.dense_shift : 31u));
-      if (P.dense_shift && Qh.split && ts - hs > thr && ld_rlx32(&G->hs_block) == 0u) {
+      const bool pull_ok = P.pull_ok && Qh.trow != nullptr && Qh.split != nullptr && !P.near_far;
+      const unsigned long long pull_thr = max(4096ull, (unsigned long long)(Qh.n >> 6));
+      if (pull_ok && pcs == 1u && ld_rlx64(&G->pc_pull) < ld_rlx64(&G->pc_push)) {
+        mode = PH_M_PULL;
+        list = PH_LSETTLED;
+        lo = 0ull;
+        hi = Qh.n;
+        if (lane == 0) st_rlx64(&G->head[PH_LSETTLED], ts);
+      } else if (pull_ok && pcs == 0u && ts - hs > pull_thr) {
+        /* count both directions on a sample of the vertices first; the
+         * settled list stays for a push */
         mode = PH_M_SCAN;
         list = PH_LSETTLED;
         lo = 0ull;
         hi = Qh.n;
+        sample = 1u;
+        pc_next = 1u;
+        if (lane == 0) {
+          st_rlx64(&G->pc_push, 0ull);
+          st_rlx64(&G->pc_pull, 0ull);
+        }
+      } else if (P.dense_shift && Qh.split && ts - hs > thr && ld_rlx32(&G->hs_block) == 0u) {
+        mode = PH_M_SCAN;
+        list = PH_LSETTLED;
+        lo = 0ull;
+        hi = Qh.n;
+        pc_next = pcs != 0u ? 2u : 0u; /* sampled already: no second sample */
         if (lane == 0) {
           st_rlx64(&G->head[PH_LSETTLED], ts);
           st_rlx32(&G->hs_block, 1u);
@@ -1169,6 +1465,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       mode = PH_M_EXIT;
     }
   }
+  if (lane == 0 && pcs != pc_next) st_rlx32(&G->pc_state, pc_next);
   const unsigned long long wb = ld_rlx64(&G->work);
   unsigned epoch = prev_epoch; /* a records-only phase keeps its producer's */
   if (lane == 0 && !hub_only) {
@@ -1217,6 +1514,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
     S.D.epoch = epoch;
     S.D.nx = nx;
     S.D.full = full;
+    S.D.sample = sample;
     for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
       S.D.xl[r] = xl[r];
       S.D.xlo[r] = xlo[r];
@@ -1252,6 +1550,28 @@ __device__ void trace_account(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   }
 }
 
+/* A phase descriptor as the leader published it (thread 0; the release of
+ * the group's generation orders it). */
+__device__ __forceinline__ void read_desc(PhDesc &D, const PhDesc *dp) {
+  D.mode = ld_rlx32(&dp->mode);
+  D.q = ld_rlx32(&dp->q);
+  D.list = ld_rlx32(&dp->list);
+  D.base = ld_rlx32(&dp->base);
+  D.lo = ld_rlx64(&dp->lo);
+  D.hi = ld_rlx64(&dp->hi);
+  D.work_base = ld_rlx64(&dp->work_base);
+  D.per = ld_rlx32(&dp->per);
+  D.epoch = ld_rlx32(&dp->epoch);
+  D.nx = ld_rlx32(&dp->nx);
+  D.full = ld_rlx32(&dp->full);
+  D.sample = ld_rlx32(&dp->sample);
+  for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
+    D.xl[r] = ld_rlx32(&dp->xl[r]);
+    D.xlo[r] = ld_rlx64(&dp->xlo[r]);
+    D.xhi[r] = ld_rlx64(&dp->xhi[r]);
+  }
+}
+
 /* frontiers small enough for the leader alone */
 template <int BLOCK, int UU>
 __device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK, UU> &S) {
@@ -1283,13 +1603,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   c.edges = 0;
   c.edges_mark = 0;
   PhGroup *G = grp_of(P, c);
-  unsigned long long cy_work = 0, cy_wait = 0, cy_lead = 0, nphase = 0;
-  const long long cy0 = clock64();
   if (tid == 0) {
+    S.cy0 = clock64();
+    S.nphase = 0ull;
     S.gen = ld_acq32(&G->gen);
     S.pcnt = 0u;
     S.D.mode = PH_M_START;
     S.D.q = 0u;
+    /* a resumed launch starts from the pull phase the last one ended with
+     * (or, when the solve is done, exits at once) */
+    if (P.resume) {
+      read_desc(S.D, &G->desc[S.gen & 1u]);
+      if (S.D.mode != PH_M_PULL) S.D.mode = PH_M_EXIT;
+    }
     S.st_items = S.st_stale = S.st_heavy = S.st_repush = S.st_pushes = S.st_chunks = 0;
     S.st_hubs = S.st_solo = 0;
     S.tr_e = S.tr_mi = S.tr_mp = 0ull;
@@ -1297,11 +1623,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   }
   if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
   __syncthreads();
-  for (;;) {
-    const long long t0 = clock64();
+  while (S.D.mode != PH_M_EXIT) { /* left at the end of the body */
+    if (tid == 0) S.tk = clock64();
     run_phase<FLT, BLOCK, UU>(P, c, S, false);
-    const long long t1 = clock64();
-    cy_work += (unsigned long long)(t1 - t0);
+    if (tid == 0) { /* run_phase as a whole, grid phases */
+      const long long t1 = clock64();
+      S.cy[6] += (unsigned long long)(t1 - S.tk);
+      S.tk = t1;
+    }
     const bool tracing = P.trace != nullptr && c.gi == 0u;
     if (tracing) trace_account<BLOCK, UU>(P, c, S);
     /* group barrier: the last CTA in becomes the leader */
@@ -1321,7 +1650,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
       for (;;) {
         if (tid < 32) leader_step<FLT, BLOCK, UU>(P, c, S);
         __syncthreads();
-        ++nphase;
+        if (tid == 0) ++S.nphase;
         if (!solo_ok<BLOCK, UU>(P, S)) break;
         if (tid == 0) {
           /* this CTA alone expands the phase; no fence: until the group is
@@ -1345,7 +1674,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
         __threadfence();
         st_rel32(&G->gen, S.gen + 1u);
       }
-      cy_lead += (unsigned long long)(clock64() - t1);
+      if (tid == 0) S.cy[5] += (unsigned long long)(clock64() - S.tk);
     } else {
       if (tid == 0) {
         Waiter w{c.deadline, 0};
@@ -1357,32 +1686,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
           }
         }
         if (ok) {
-          const PhDesc *dp = &G->desc[(S.gen + 1u) & 1u];
-          S.D.mode = ld_rlx32(&dp->mode);
-          S.D.q = ld_rlx32(&dp->q);
-          S.D.list = ld_rlx32(&dp->list);
-          S.D.base = ld_rlx32(&dp->base);
-          S.D.lo = ld_rlx64(&dp->lo);
-          S.D.hi = ld_rlx64(&dp->hi);
-          S.D.work_base = ld_rlx64(&dp->work_base);
-          S.D.per = ld_rlx32(&dp->per);
-          S.D.epoch = ld_rlx32(&dp->epoch);
-          S.D.nx = ld_rlx32(&dp->nx);
-          S.D.full = ld_rlx32(&dp->full);
-          for (unsigned r = 0; r < PH_MAXR - 1; ++r) {
-            S.D.xl[r] = ld_rlx32(&dp->xl[r]);
-            S.D.xlo[r] = ld_rlx64(&dp->xlo[r]);
-            S.D.xhi[r] = ld_rlx64(&dp->xhi[r]);
-          }
+          read_desc(S.D, &G->desc[(S.gen + 1u) & 1u]);
         } else {
           S.D.mode = PH_M_EXIT;
         }
       }
-      cy_wait += (unsigned long long)(clock64() - t1);
+      if (tid == 0) S.cy[4] += (unsigned long long)(clock64() - S.tk);
     }
     if (tid == 0) ++S.gen;
     __syncthreads();
-    if (S.D.mode == PH_M_EXIT) break;
+    /* a pull phase ends the launch: the pull kernel runs it, and the next
+     * launch (resume) continues from its descriptor */
+    if (S.D.mode == PH_M_EXIT || S.D.mode == PH_M_PULL) break;
   }
   /* statistics */
   PhGlobal *g = P.g;
@@ -1398,12 +1713,63 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     atomicAdd(&g->st_chunks, S.st_chunks);
     atomicAdd(&g->st_hub, S.st_hubs);
     atomicAdd(&g->st_solo, S.st_solo);
-    atomicAdd(&g->st_phases, nphase);
-    S.cy[4] = cy_wait;
-    S.cy[5] = cy_lead;
-    S.cy[6] = cy_work; /* run_phase as a whole, grid phases */
-    S.cy[7] = (unsigned long long)(clock64() - cy0);
+    atomicAdd(&g->st_phases, S.nphase);
+    S.cy[7] = (unsigned long long)(clock64() - S.cy0);
     for (int i = 0; i < 8; ++i) atomicAdd(&g->st_cyc[i], S.cy[i]);
+  }
+}
+
+/* The pull phase of a one-query launch chain (PH_M_PULL), in a kernel of its
+ * own so that the phase kernel's push loop keeps its registers (the same
+ * loop instantiated twice in one kernel, or called out of it, made the push
+ * loop up to 40 % slower on R-MAT 24).  Its CTAs are co-resident like the
+ * phase kernel's (a list reservation may wait for another CTA's page
+ * mapping) and claim vertex tiles until none is left.  A launch with no pull
+ * to run -- the solve has ended, or failed -- returns at once. */
+template <bool FLT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) pull_kernel(const __grid_constant__ PhParams P) {
+  constexpr int UU = PH_U(BLOCK, MINB);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PSmem<BLOCK, UU> &S = *reinterpret_cast<PSmem<BLOCK, UU> *>(smem_raw);
+  const unsigned tid = threadIdx.x;
+  Ctx c;
+  c.gi = 0u; /* one query, one group */
+  c.rank = blockIdx.x;
+  c.deadline = gtimer() + P.timeout_ns;
+  c.edges = 0;
+  c.edges_mark = 0;
+  PhGroup *G = grp_of(P, c);
+  if (tid == 0) {
+    read_desc(S.D, &G->desc[ld_acq32(&G->gen) & 1u]);
+    if (ld_rlx32(&P.g->err) != 0u) S.D.mode = PH_M_EXIT;
+    S.pcnt = 0u;
+    S.st_items = S.st_stale = S.st_heavy = S.st_repush = S.st_pushes = S.st_chunks = 0;
+    S.st_hubs = S.st_solo = 0;
+    S.tr_e = S.tr_mi = S.tr_mp = 0ull;
+    S.pend = ~0ull;
+    S.pl_k = 0u;
+  }
+  if (tid < PH_NLIST) S.ptc_vp[tid] = ~0ull;
+  __syncthreads();
+  if (S.D.mode != PH_M_PULL) return;
+  const PhQuery &Q = P.qs[S.D.q];
+  if (tid == 0) S.pl_T = pull_floor<FLT>(Q, S.D.base); /* read after prepare's barrier */
+  while (prepare_pull<FLT, BLOCK, UU>(P, c, S, Q)) {
+    pull_tile_warp<FLT, BLOCK, UU>(P, c, S, Q);
+    __syncthreads();
+    if (tid == 0) ++S.st_chunks;
+    if (S.pcnt > PSmem<BLOCK, UU>::FLUSH_AT) flush<BLOCK, UU>(P, c, S);
+  }
+  flush<BLOCK, UU>(P, c, S);
+  if (P.trace != nullptr) trace_account<BLOCK, UU>(P, c, S);
+  PhGlobal *g = P.g;
+  unsigned long long s_edges = c.edges;
+  for (int o = 16; o > 0; o >>= 1) s_edges += __shfl_down_sync(0xFFFFFFFFu, s_edges, o);
+  if ((tid & 31u) == 0u && s_edges) atomicAdd(&g->st_edges, s_edges);
+  if (tid == 0) {
+    atomicAdd(&g->st_items, S.st_items);
+    atomicAdd(&g->st_pushes, S.st_pushes);
+    atomicAdd(&g->st_chunks, S.st_chunks);
   }
 }
 
@@ -1413,14 +1779,18 @@ static cudaError_t prep_one(int *max_blocks_per_sm) {
   cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(pull_kernel<FLT, BLOCK, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
                                                        phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
 }
 
 template <bool FLT, int BLOCK, int MINB>
-static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
+static cudaError_t launch_one(const PhParams &P, cudaStream_t st, bool pull) {
   /* cooperative launch: every CTA of a group waits at the group barrier, so
-   * all of them must be resident; the Ex form keeps it graph-capturable */
+   * all of them must be resident; the Ex form keeps it graph-capturable.
+   * The pull kernel takes the same grid. */
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P.groups * P.gsize);
   cfg.blockDim = dim3(BLOCK);
@@ -1431,7 +1801,8 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB>, P);
+  return pull ? cudaLaunchKernelEx(&cfg, pull_kernel<FLT, BLOCK, MINB>, P)
+              : cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB>, P);
 }
 
 /* Failure-detection check: thread 0 waits, through the same bounded Waiter
@@ -1507,10 +1878,11 @@ cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm) {
   return cudaErrorInvalidValue;
 }
 
-cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st) {
+cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st, bool pull) {
   using namespace adds_phase;
 #define X(i, b, m) \
-  if (variant == i) return P.is_float ? launch_one<true, b, m>(P, st) : launch_one<false, b, m>(P, st);
+  if (variant == i)  \
+    return P.is_float ? launch_one<true, b, m>(P, st, pull) : launch_one<false, b, m>(P, st, pull);
   PH_VARIANTS(X)
 #undef X
   return cudaErrorInvalidValue;
@@ -1682,6 +2054,9 @@ int ph_engine_params(const PhEngine &E, const PhKnobs &k, unsigned single_src, P
   P->near_far = k.near_far ? 1u : 0u;
   P->dense_shift = k.near_far ? 0u : k.dense_shift;
   P->is_float = E.flt ? 1u : 0u;
+  /* pull phases: one query on one group, with an in-edge CSR */
+  P->pull_ok = (E.nq == 1 && E.groups == 1 && E.qs_host[0].trow != nullptr) ? 1u : 0u;
+  P->resume = 0u;
   P->single_src = single_src;
   P->timeout_ns = k.timeout_ns;
   P->trace = E.trace;
@@ -1720,6 +2095,20 @@ int ph_engine_enqueue(PhEngine &E, const PhParams &P, cudaStream_t st, cudaEvent
     return -5;
   if (k0 && cudaEventRecordWithFlags(k0, st, fl) != cudaSuccess) return -5;
   if (adds_phase_launch(P, (int)E.variant, st) != cudaSuccess) return -5;
+  if (P.pull_ok) {
+    /* a launch that picks a pull phase ends there; each pull kernel runs the
+     * phase the launch before it ended with, and the next launch resumes
+     * from it.  The last launch picks no pull, so the chain always finishes
+     * the solve; launches with nothing left to do return at once. */
+    PhParams R = P;
+    R.resume = 1u;
+    for (unsigned s = 1; s <= PH_PULL_SEGMENTS; ++s) {
+      R.pull_ok = s < PH_PULL_SEGMENTS ? 1u : 0u;
+      if (adds_phase_launch(R, (int)E.variant, st, true) != cudaSuccess ||
+          adds_phase_launch(R, (int)E.variant, st) != cudaSuccess)
+        return -5;
+    }
+  }
   if (k1 && cudaEventRecordWithFlags(k1, st, fl) != cudaSuccess) return -5;
   if (cudaMemcpyAsync(E.g_host, E.g, sizeof(PhGlobal), cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return -5;

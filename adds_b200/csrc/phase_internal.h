@@ -39,6 +39,8 @@
 #define PH_M_HUB 3u    /* (reserved: split rows are expanded inside their phase) */
 #define PH_M_EXIT 4u   /* no more queries for this group                      */
 #define PH_M_SCAN 6u   /* collect a dense bucket from the distances into NEXT  */
+#define PH_M_PULL 7u   /* heavy phase as a pull: every vertex above the bucket
+                          takes the minimum over its in-edges                */
 
 /* device error codes (first one wins) */
 #define PH_ERR_TIMEOUT 1u
@@ -60,6 +62,10 @@ struct PhQuery {
   float scale;           /* float graphs: key = floor(d * scale)              */
   unsigned shift;        /* bucket = key >> shift                             */
   unsigned long long m;
+  /* in-edge CSR (the transposed graph: {tail vertex, weight bits} per edge)
+   * for heavy phases run as a pull; NULL = push only */
+  const unsigned *trow;
+  const uint2 *tedges;
 };
 
 /* One split-row chunk: edges [eb, ee) of vertex v expanded with distance d. */
@@ -70,6 +76,10 @@ struct __align__(16) PhHub {
 /* What every CTA of a group needs for one phase (written by the leader before
  * it releases the barrier; double-buffered by barrier generation). */
 #define PH_MAXR 4 /* list ranges one light phase may read (widened bucket) */
+/* launches of the phase kernel one solve may be split into by pull phases
+ * (each pull runs in a kernel between two of them) */
+#define PH_PULL_SEGMENTS 2u
+#define PH_SAMPLE_STRIDE 16u /* a sampling heavy scan reads every 16th tile */
 struct __align__(64) PhDesc {
   unsigned mode;
   unsigned q;                  /* query index                                */
@@ -85,7 +95,9 @@ struct __align__(64) PhDesc {
   unsigned xl[PH_MAXR - 1];
   unsigned long long xlo[PH_MAXR - 1], xhi[PH_MAXR - 1];
   unsigned full;               /* light phase relaxes whole rows, no SETTLED */
-  unsigned pad[3];
+  unsigned sample;             /* heavy scan that only counts push and pull
+                                  work, over one tile in PH_SAMPLE_STRIDE  */
+  unsigned pad[2];
 };
 
 /* Per-group state.  `arrive` and `gen` sit in lines of their own; the list
@@ -132,7 +144,15 @@ struct __align__(128) PhGroup {
    * scan: it was already, or a light phase relaxed whole rows, or the
    * bucket was widened over several slots */
   unsigned hs_block;
-  unsigned pad5[13];
+  /* pull or push for a settled bucket's heavy edges: a sampling heavy scan
+   * sums the heavy out-edges of the bucket (pc_push) and the in-edges of
+   * every vertex a heavy edge could still improve (pc_pull) over the same
+   * sample; pc_state is 1 while those sums belong to the decision about to
+   * be made, 2 right after it chose push (no second sample) */
+  unsigned pc_state;
+  unsigned pad5[12];
+  unsigned long long pc_push, pc_pull;
+  unsigned long long pad5b[14];
   /* dense bucket slots (bit per slot): a slot whose pushes passed the dense
    * threshold stops storing entries; its bucket is collected by a scan of
    * the distances when it opens (PH_M_SCAN) */
@@ -202,6 +222,11 @@ struct PhParams {
                                   max(n >> dense_shift, 4096) pushes turns
                                   dense (collected by a scan); 0 = never      */
   unsigned is_float;
+  /* pull phases (one query per launch): the leader may pick PH_M_PULL,
+   * which ends this launch; the pull kernel runs the phase and a launch
+   * with resume = 1 continues from its descriptor */
+  unsigned pull_ok;
+  unsigned resume;
   unsigned single_src;         /* overrides query 0's source when != ~0       */
   unsigned long long timeout_ns;
   PhTrace *trace;              /* optional phase trace of group 0              */
@@ -250,7 +275,8 @@ struct PhKnobs {
 /* phase.cu host API (C++ linkage) */
 int adds_phase_variant_block(int variant);
 cudaError_t adds_phase_prepare(bool flt, int variant, int *max_blocks_per_sm);
-cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st);
+/* pull = true launches the pull kernel of a launch chain (ph_engine_enqueue) */
+cudaError_t adds_phase_launch(const PhParams &P, int variant, cudaStream_t st, bool pull = false);
 int ph_engine_alloc(PhEngine &E, int device, bool flt, const std::vector<PhQuery> &qv,
                     const PhKnobs &k, unsigned grow, cudaStream_t st);
 void ph_engine_free(PhEngine &E);

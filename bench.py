@@ -416,7 +416,7 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
                                                         "hub_threshold", "light_heavy", "window",
                                                         "batch_max", "strict_order", "adapt",
                                                         "local_max", "greed", "group_ctas",
-                                                        "dense_scan")}
+                                                        "dense_scan", "pull")}
                       if tuned else None),
             "lib": os.path.relpath(A._lib.LIB_PATH, ROOT),
             "tune_ms_per_solve": tune_ms,

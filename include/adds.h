@@ -107,7 +107,15 @@ typedef struct adds_opts {
                             the distances when it opens (no duplicate or stale
                             entries); 0 = auto (off unless tuned), < 0 = off,
                             6 = n/64                                        */
-  int32_t reserved[3];
+  int32_t pull;          /* phase engine, light/heavy split on: the heavy edges
+                            of a large settled bucket may be relaxed as a pull
+                            -- every vertex they could still improve takes the
+                            minimum over its in-edges -- when a count over the
+                            distances finds that this reads fewer edges than
+                            the push.  Keeps a transposed copy of the graph
+                            (8 B per edge, built on first use).  0 = auto
+                            (on), < 0 = off, 1 = on                         */
+  int32_t reserved[2];
 } adds_opts;
 
 /* Engines.  PHASE settles the buckets in bulk-synchronous phases (light

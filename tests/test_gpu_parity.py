@@ -323,6 +323,87 @@ def test_adaptive_light_heavy_saves_phases():
     assert st[2]["edges_scanned"] <= 1.05 * st[1]["edges_scanned"]
 
 
+def _pull_phases(g, src, **kw):
+    """Distances, statistics and the number of pull phases of one solve."""
+    dg = A.Graph.from_csr(g)
+    try:
+        dg.trace(1 << 14)
+        d, st = dg.sssp(src, A.default_opts(**{**OPTS, **kw}))
+        tr, _ = dg.trace_read(1 << 14)
+        dg.trace(0)
+    finally:
+        dg.close()
+    ref, _ = O.dijkstra(g, src)
+    mism = np.flatnonzero(d != ref)
+    assert mism.size == 0, f"{mism.size} mismatches, first {mism[:5]} got {d[mism[:5]]} want {ref[mism[:5]]}"
+    return st, int(((tr["mode"] & 0xFF) == 7).sum())
+
+
+@pytest.mark.parametrize("variant", [(256, 4), (1024, 1), (128, 8)])
+def test_pull_heavy_phase_int_rmat(variant):
+    """A giant bucket's heavy edges taken as a pull over the in-edges of the
+    vertices above it (R-MAT, int weights U[1, 10000), bucket 2^10): a pull
+    phase runs, the distances equal the oracle's, and fewer edges are read
+    than with pushes only (pull = -1)."""
+    g = G.rmat(17, 16, seed=41, w_hi=10000)
+    src = G.max_degree_vertex(g)
+    kw = dict(engine=PHASE, delta_shift=10, light_heavy=1, block_threads=variant[0],
+              ctas_per_sm=variant[1])
+    st_pull, npull = _pull_phases(g, src, pull=1, **kw)
+    st_push, npush = _pull_phases(g, src, pull=-1, **kw)
+    assert npull >= 1 and npush == 0
+    assert st_pull["edges_scanned"] < st_push["edges_scanned"]
+
+
+@pytest.mark.parametrize("lh", [1, 2])
+def test_pull_heavy_phase_float(lh):
+    """Float keys (the rounded lower bound of a heavy candidate): R-MAT with
+    float weights and a float grid, pull on and off, equal to the oracle."""
+    g = G.rmat(16, 16, seed=43, wtype=G.F32, w_lo=0.0, w_hi=1.0)
+    src = G.max_degree_vertex(g)
+    for shift in (4, 8, 12):
+        _pull_phases(g, src, engine=PHASE, delta_shift=shift, light_heavy=lh, pull=1)
+    gg = G.grid(128, 128, 0.02, 8, wtype=G.F32, w_lo=0.0, w_hi=3.0, seed=44)
+    for shift in (8, 14):
+        _pull_phases(gg, 64 * 128 + 64, engine=PHASE, delta_shift=shift, light_heavy=lh, pull=1)
+
+
+def test_pull_after_weight_update_and_in_batch():
+    """The in-edge copy follows adds_graph_set_weights; a batch of one query
+    replays the launch chain of a pulled solve from its CUDA graph (twice),
+    and a batch of several stays on pushes; all equal the oracle."""
+    g = G.rmat(15, 16, seed=45, w_hi=10000)
+    src = G.max_degree_vertex(g)
+    dg = A.Graph.from_csr(g)
+    try:
+        o = A.default_opts(**OPTS, engine=PHASE, delta_shift=10, pull=1)
+        d0, _ = dg.sssp(src, o)
+        assert np.array_equal(d0, O.dijkstra(g, src)[0])
+        w2 = (np.random.default_rng(7).integers(1, 10000, size=g.w.size)).astype(np.uint32)
+        dg.set_weights(w2)
+        d1, _ = dg.sssp(src, o)
+        assert np.array_equal(d1, O.dijkstra(G.CSR(g.n, g.row, g.dst, w2, g.wtype), src)[0])
+    finally:
+        dg.close()
+    graphs = [G.rmat(15, 16, seed=46 + i, w_hi=10000) for i in range(3)]
+    dgs = [A.Graph.from_csr(x) for x in graphs]
+    srcs = [G.max_degree_vertex(x) for x in graphs]
+    try:
+        for k in (1, 3):
+            b = A.Batch(dgs[:k], srcs[:k],
+                        A.default_opts(**OPTS, engine=PHASE, delta_shift=10, pull=1))
+            try:
+                for _ in range(2):
+                    b.run()
+                    for q, (x, s) in enumerate(zip(graphs[:k], srcs[:k])):
+                        assert np.array_equal(b.dist(q), O.dijkstra(x, s)[0])
+            finally:
+                b.close()
+    finally:
+        for x in dgs:
+            x.close()
+
+
 def test_phase_float_grid_large_keys():
     """A high-diameter float grid with a narrow bucket (many slots, far-slot
     re-pushes) and zero-weight edges mixed in."""
