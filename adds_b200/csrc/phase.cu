@@ -140,7 +140,8 @@ __device__ __forceinline__ unsigned route(unsigned b, unsigned base, unsigned ne
 /* shared memory of one CTA                                                   */
 #define PH_RES_PAGES 6u /* pages one list reservation may touch (flush size) */
 #define PH_EPT 1        /* frontier entries one thread prepares per chunk     */
-#define PH_PULL_V 4u    /* vertices one thread selects per pull tile          */
+#define PH_PULL_V 4u    /* vertices one thread selects per pull sub-tile      */
+#define PH_PULL_SUB 2u  /* pull sub-tiles per block barrier                  */
 /* split-row chunk records one CTA takes at a time */
 #define PH_HUB_PER_CLAIM(BLOCK) ((BLOCK) / 16u)
 
@@ -831,14 +832,14 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
  * this phase.  The direction choice follows Beamer et al. (SC 2012), applied
  * to delta-stepping's heavy phase as in Chakaravarthy et al. (IPDPS 2014).
  *
- * CTAs claim runs of tiles of PH_PULL_V x BLOCK vertices (guided
+ * CTAs claim runs of tiles of PH_PULL_SUB x PH_PULL_V x BLOCK vertices (guided
  * self-scheduling, the next run claimed one run ahead; thread 0 keeps the
  * runs in shared memory) and run each through pull_tile.  Claims the next
  * tile into S.pl_cur; false when none is left.  Every thread calls it. */
 template <bool FLT, int BLOCK, int UU>
 __device__ bool prepare_pull(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q) {
   const unsigned tid = threadIdx.x;
-  const unsigned long long tv = (unsigned long long)PH_PULL_V * BLOCK;
+  const unsigned long long tv = (unsigned long long)PH_PULL_SUB * PH_PULL_V * BLOCK;
   const unsigned ntile = (unsigned)(((unsigned long long)Q.n + tv - 1ull) / tv);
   __syncthreads(); /* everyone has read the previous tile's S.pl_cur and S.stop */
   if (tid == 0) {
@@ -878,8 +879,9 @@ __device__ __forceinline__ unsigned warp_incl_scan(unsigned x) {
   return x;
 }
 
-/* One claimed pull tile, PH_PULL_V x BLOCK consecutive vertices, each warp
- * on its own 32 x PH_PULL_V of them with no block barrier (the block-wide
+/* Sub-tile `sub` of a claimed pull tile (PH_PULL_SUB sub-tiles of PH_PULL_V
+ * x BLOCK consecutive vertices, run before one block barrier), each warp on
+ * its own 32 x PH_PULL_V of them with no block barrier (the block-wide
  * version spent 40 % of its issue slots waiting at barriers).  A lane
  * selects its vertices above pull_floor that have in-edges; the warp
  * compacts them into its 32-item slice of the chunk arrays, 32 at a time,
@@ -893,18 +895,19 @@ __device__ __forceinline__ unsigned warp_incl_scan(unsigned x) {
  * check. */
 template <bool FLT, int BLOCK, int UU>
 __device__ void pull_tile_warp(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S,
-                               const PhQuery &Q) {
+                               const PhQuery &Q, unsigned sub) {
   constexpr unsigned V = PH_PULL_V, U = PSmem<BLOCK, UU>::U, R = 32u * U;
   constexpr unsigned SB = PSmem<BLOCK, UU>::SB, FLUSH_AT = PSmem<BLOCK, UU>::FLUSH_AT;
   static_assert(PSmem<BLOCK, UU>::IC == BLOCK, "one 32-item slice per warp");
-  static_assert(FLUSH_AT + V * BLOCK <= SB, "a tile's pushes fit the staging buffer");
+  static_assert(FLUSH_AT + PH_PULL_SUB * V * BLOCK <= SB, "a tile's pushes fit the staging buffer");
   const unsigned tid = threadIdx.x, lane = tid & 31u, sl = tid & ~31u;
   unsigned *const w_rb = S.it_rb + sl, *const w_best = S.it_du + sl, *const w_d0 = S.it_d0 + sl;
   unsigned *const w_v = S.it_v + sl, *const w_off = S.it_off + sl;
   const uint2 *__restrict__ edges = Q.tedges;
   unsigned *const dist = Q.dist;
   const unsigned n = Q.n, T = S.pl_T;
-  const unsigned long long v0 = ((unsigned long long)S.pl_cur * BLOCK + tid) * V;
+  const unsigned long long v0 =
+      (((unsigned long long)S.pl_cur * PH_PULL_SUB + sub) * BLOCK + tid) * V;
   unsigned d[V], rb[V], re[V];
   const bool vec = ((reinterpret_cast<unsigned long long>(Q.dist) |
                      reinterpret_cast<unsigned long long>(Q.trow)) & 15ull) == 0ull;
@@ -1755,7 +1758,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) pull_kernel(const __grid_constant
   const PhQuery &Q = P.qs[S.D.q];
   if (tid == 0) S.pl_T = pull_floor<FLT>(Q, S.D.base); /* read after prepare's barrier */
   while (prepare_pull<FLT, BLOCK, UU>(P, c, S, Q)) {
-    pull_tile_warp<FLT, BLOCK, UU>(P, c, S, Q);
+    for (unsigned sub = 0; sub < PH_PULL_SUB; ++sub) pull_tile_warp<FLT, BLOCK, UU>(P, c, S, Q, sub);
     __syncthreads();
     if (tid == 0) ++S.st_chunks;
     if (S.pcnt > PSmem<BLOCK, UU>::FLUSH_AT) flush<BLOCK, UU>(P, c, S);
