@@ -87,7 +87,8 @@ class Stats(C.Structure):
         ("retries", C.c_int32),
         ("ctas", C.c_int32),
         ("engine", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("launches", C.c_int32),
+        ("reserved", C.c_int32 * 3),
         ("phases", C.c_uint64),
         ("solo_phases", C.c_uint64),
         ("repushes", C.c_uint64),

@@ -379,6 +379,7 @@ static void fill_stats(const Engine &E, const EngParams &P, adds_stats *s) {
   s->mid_flush_cycles = g.st_pad[0];
   s->mid_flushes = g.st_pad[1];
   s->ctas = (int32_t)P.nctas;
+  s->launches = 2; /* init kernel, persistent solver */
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1354,6 +1355,9 @@ static void fill_phase_stats(const PhEngine &E, adds_stats *s) {
   s->mid_flushes = g.st_cyc[7];      /* total */
   s->ctas = (int32_t)(E.groups * E.gsize);
   s->engine = ADDS_ENGINE_PHASE;
+  /* the launch chain of ph_engine_enqueue when pull phases are possible */
+  const bool chain = E.nq == 1 && E.groups == 1 && E.qs_host[0].trow != nullptr;
+  s->launches = chain ? (int32_t)(1u + 2u * PH_PULL_SEGMENTS) : 1;
   s->phases = g.st_phases;
   s->solo_phases = g.st_solo;
   s->repushes = g.st_repush;

@@ -389,16 +389,18 @@ def run_ours(args, wl_name, wl, ws, rank, local, dist):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
-                     "kernel": ("adds_phase::phase_kernel" if st["engine"] == 2 else
-                                "adds::solve_kernel") + " (persistent, 1 launch per solve)",
+                     "kernel": ("adds_phase::phase_kernel (+ pull_kernel)" if st["engine"] == 2
+                                else "adds::solve_kernel")
+                               + f" (persistent, {st['launches']} launches per solve)",
                      "traffic_note": (prof or {}).get("scaled_by"),
                      "dram_gbs": (traffic / (kernel_s / args.steps) / 1e9) if traffic else None,
                      "l2_hit_rate_pct": (prof or {}).get("l2_hit_rate_pct"),
                      "bytes_model": "12*m_r + 24*n_r per solve"},
         "e2e": e2e,
-        # phase engine: one persistent kernel per solve; asynchronous engine:
-        # its init kernel and its persistent kernel
-        "gpu_launches": (1 if st["engine"] == 2 else 2) * args.steps,
+        # phase engine: one persistent kernel per solve, or a chain of five
+        # (phase, pull, phase, pull, phase) where pull phases are possible;
+        # asynchronous engine: its init kernel and its persistent kernel
+        "gpu_launches": st["launches"] * args.steps,
         "clocks": clocks,
         "extra": {
             "n": g.n, "m": g.m, "sources": srcs, "m_r": [mr[s] for s in srcs],
@@ -609,7 +611,7 @@ def run_batched(args, ws, rank, local, dist):
         "e2e": {"value": 256 / e2e_max, "unit": "solves/s",
                 "h2d_bytes_per_step": 4 * len(qs), "d2h_bytes_per_step": 4 * tot_n,
                 "gathered_words_on_rank0": gathered},
-        "gpu_launches": (1 if st["engine"] == 2 else 2) * args.steps, "clocks": clocks,
+        "gpu_launches": st["launches"] * args.steps, "clocks": clocks,
         "extra": {"kernel_ms_per_launch": kms / args.steps},
     }
     b.close()

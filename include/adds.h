@@ -153,7 +153,11 @@ typedef struct adds_stats {
   int32_t retries;          /* worklist regrowths needed                       */
   int32_t ctas;             /* persistent CTAs launched                        */
   int32_t engine;           /* ADDS_ENGINE_ASYNC or ADDS_ENGINE_PHASE          */
-  int32_t reserved[4];
+  int32_t launches;         /* kernel launches per solve: async 2 (init, solver);
+                               phase 1, or 5 with pull phases possible (phase,
+                               pull, phase, pull, phase; unused ones return at
+                               once)                                         */
+  int32_t reserved[3];
   uint64_t phases;          /* phase engine: phases decided (solo included)    */
   uint64_t solo_phases;     /* phase engine: phases run by one CTA             */
   uint64_t repushes;        /* phase engine: far-slot entries moved on         */

@@ -42,12 +42,12 @@ def test_every_declared_function_is_exported():
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "adds.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", '
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", '
                    'sizeof(adds_opts), sizeof(adds_stats), sizeof(adds_graph_info_t), '
                    'sizeof(adds_gen_spec), offsetof(adds_stats, phase_cycles), '
                    'offsetof(adds_opts, solo_max), offsetof(adds_opts, near_far), '
                    'offsetof(adds_stats, repushes), offsetof(adds_opts, dense_scan), '
-                   'offsetof(adds_opts, pull));return 0;}\n')
+                   'offsetof(adds_opts, pull), offsetof(adds_stats, launches));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
                    check=True)
@@ -55,7 +55,8 @@ def test_struct_layouts_match_c(tmp_path):
                                           check=True).stdout.split()]
     want = [C.sizeof(L.Opts), C.sizeof(L.Stats), C.sizeof(L.GraphInfo), C.sizeof(L.GenSpec),
             L.Stats.phase_cycles.offset, L.Opts.solo_max.offset, L.Opts.near_far.offset,
-            L.Stats.repushes.offset, L.Opts.dense_scan.offset, L.Opts.pull.offset]
+            L.Stats.repushes.offset, L.Opts.dense_scan.offset, L.Opts.pull.offset,
+            L.Stats.launches.offset]
     assert got == want
 
 

@@ -353,6 +353,8 @@ def test_pull_heavy_phase_int_rmat(variant):
     st_push, npush = _pull_phases(g, src, pull=-1, **kw)
     assert npull >= 1 and npush == 0
     assert st_pull["edges_scanned"] < st_push["edges_scanned"]
+    # the launch chain (phase, pull, phase, pull, phase) against one launch
+    assert st_pull["launches"] == 5 and st_push["launches"] == 1
 
 
 @pytest.mark.parametrize("lh", [1, 2])
