@@ -1285,9 +1285,12 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         lo = 0ull;
         hi = Qh.n;
         if (lane == 0) st_rlx64(&G->head[PH_LSETTLED], ts);
-      } else if (pull_ok && pcs == 0u && ts - hs > pull_thr) {
+      } else if (pull_ok && pcs == 0u && ts - hs > pull_thr && ld_rlx32(&G->hs_block) == 0u) {
         /* count both directions on a sample of the vertices first; the
-         * settled list stays for a push */
+         * settled list stays for a push.  Only for a settled list of one
+         * bucket (hs_block clear): after a widened light phase it holds
+         * vertices of lower buckets too, whose heavy edges can reach
+         * vertices at or below pull_floor, which a pull does not visit */
         mode = PH_M_SCAN;
         list = PH_LSETTLED;
         lo = 0ull;

@@ -357,6 +357,31 @@ def test_pull_heavy_phase_int_rmat(variant):
     assert st_pull["launches"] == 5 and st_push["launches"] == 1
 
 
+@pytest.mark.parametrize("solo", [0, 1024])
+@pytest.mark.parametrize("adapt", [0, 1])
+def test_pull_with_widened_buckets(adapt, solo):
+    """Pull phases next to on-device bucket widening: a widened light phase
+    leaves vertices of several buckets in the settled list, whose heavy
+    edges a pull above the top bucket would miss -- those lists go to a
+    push.  Eight sources of an R-MAT with narrow buckets, each equal to the
+    oracle."""
+    g = G.rmat(17, 16, seed=47, w_hi=10000)
+    deg = np.diff(g.row.astype(np.int64))
+    srcs = [int(x) for x in np.random.default_rng(47).choice(np.flatnonzero(deg > 0), 8,
+                                                              replace=False)]
+    dg = A.Graph.from_csr(g)
+    try:
+        o = A.default_opts(**OPTS, engine=PHASE, delta_shift=9, light_heavy=2, adapt=adapt,
+                           solo_max=solo, pull=1)
+        for s in srcs:
+            d, _ = dg.sssp(s, o)
+            ref, _ = O.dijkstra(g, s)
+            mism = np.flatnonzero(d != ref)
+            assert mism.size == 0, f"source {s}: {mism.size} mismatches"
+    finally:
+        dg.close()
+
+
 @pytest.mark.parametrize("lh", [1, 2])
 def test_pull_heavy_phase_float(lh):
     """Float keys (the rounded lower bound of a heavy candidate): R-MAT with
