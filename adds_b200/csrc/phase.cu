@@ -161,8 +161,6 @@ struct PSmem {
   unsigned it_rb[IC];
   unsigned it_du[IC];      /* distance the item is expanded with                 */
   unsigned it_off[IC + 1]; /* exclusive scan of the segment lengths              */
-  unsigned it_d0[IC];      /* pull batch: each vertex's distance before it       */
-  unsigned it_v[IC];       /* pull batch: the item's vertex                      */
   unsigned ck_k, ck_E;        /* items and edges of the chunk                    */
   unsigned pb_v[SB];
   unsigned pb_d[SB];
@@ -182,15 +180,18 @@ struct PSmem {
                                waits), expand, flush, barrier wait, leader,
                                grid-phase work, total */
   unsigned total, pcnt, leader, gen, pi0, pi1, stop;
-  /* pull phase: next tile of the current run, tiles left in it, the tile
-   * being expanded, pull_floor of the phase's bucket */
-  unsigned pl_t0, pl_k, pl_cur, pl_T;
+  unsigned hub_made; /* this CTA cut a row into records in the current phase */
+  unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
+  /* -- after the fields above, which keep their offsets -- */
   /* thread 0's claim state and cycle marks (kept here, not in registers) */
   unsigned long long local_claim, pend;
   long long tph, tk, cy0;
   unsigned long long nphase;
-  unsigned hub_made; /* this CTA cut a row into records in the current phase */
-  unsigned long long tr_e, tr_mi, tr_mp; /* trace: phase edges, counter marks */
+  /* pull phase: next tile of the current run, tiles left in it, the tile
+   * being expanded, pull_floor of the phase's bucket */
+  unsigned pl_t0, pl_k, pl_cur, pl_T;
+  unsigned it_d0[IC]; /* pull batch: each vertex's distance before it */
+  unsigned it_v[IC];  /* pull batch: the item's vertex                 */
 };
 
 /* thread 0's cycle accounting: the cycles since the last mark go to cy[i] */
@@ -1197,10 +1198,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   unsigned nx = 0, xl[PH_MAXR - 1] = {0u, 0u, 0u}, full = 0u;
   unsigned long long xlo[PH_MAXR - 1] = {0ull, 0ull, 0ull}, xhi[PH_MAXR - 1] = {0ull, 0ull, 0ull};
   bool decide = false, next_query = false;
-  /* the heavy scan that just ran counted push and pull work (read once: the
-   * flag holds for this decision only) */
-  const unsigned pcs = ld_rlx32(&G->pc_state);
-  unsigned pc_next = 0u, sample = 0u;
+  unsigned sample = 0u; /* a heavy scan that only counts (pull or push) */
   if (ld_rlx32(&P.g->err) != 0u) {
     mode = PH_M_EXIT;
   } else if (prev_mode == PH_M_START) {
@@ -1225,6 +1223,8 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       st_rlx64(&G->dmask, 0ull);
       st_rlx64(&G->fmask, 0ull);
       st_rlx32(&G->hs_block, 0u);
+      st_rlx32(&G->pc_state, 0u);
+      st_rlx32(&G->wide, 0u);
       __threadfence();
     }
     __syncwarp();
@@ -1279,18 +1279,25 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       const unsigned long long thr = max(4096u, Qh.n >> (P.dense_shift ? P.dense_shift : 31u));
       const bool pull_ok = P.pull_ok && Qh.trow != nullptr && Qh.split != nullptr && !P.near_far;
       const unsigned long long pull_thr = max(4096ull, (unsigned long long)(Qh.n >> 6));
-      if (pull_ok && pcs == 1u && ld_rlx64(&G->pc_pull) < ld_rlx64(&G->pc_push)) {
+      /* 1: the sampling scan just counted for this list; 2: it chose push
+       * (no second sample).  Read only where a pull is possible. */
+      const unsigned pcs = pull_ok ? ld_rlx32(&G->pc_state) : 0u;
+      /* a settled list of one bucket: after a widened light phase it holds
+       * vertices of lower buckets too, whose heavy edges can reach vertices
+       * at or below pull_floor, which a pull does not visit.  (A light phase
+       * that relaxed whole rows is no obstacle: it re-relaxes nothing a pull
+       * would miss.) */
+      const bool one_bucket = pull_ok && ld_rlx32(&G->wide) == 0u;
+      unsigned pc_next = 0u;
+      if (one_bucket && pcs == 1u && ld_rlx64(&G->pc_pull) < ld_rlx64(&G->pc_push)) {
         mode = PH_M_PULL;
         list = PH_LSETTLED;
         lo = 0ull;
         hi = Qh.n;
         if (lane == 0) st_rlx64(&G->head[PH_LSETTLED], ts);
-      } else if (pull_ok && pcs == 0u && ts - hs > pull_thr && ld_rlx32(&G->hs_block) == 0u) {
+      } else if (one_bucket && pcs == 0u && ts - hs > pull_thr) {
         /* count both directions on a sample of the vertices first; the
-         * settled list stays for a push.  Only for a settled list of one
-         * bucket (hs_block clear): after a widened light phase it holds
-         * vertices of lower buckets too, whose heavy edges can reach
-         * vertices at or below pull_floor, which a pull does not visit */
+         * settled list stays for a push */
         mode = PH_M_SCAN;
         list = PH_LSETTLED;
         lo = 0ull;
@@ -1317,6 +1324,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
         lo = hs;
         hi = ts;
       }
+      if (lane == 0 && pcs != pc_next) st_rlx32(&G->pc_state, pc_next);
     } else if (P.near_far) {
       /* near-far: the threshold moves up one bucket, or to the smallest
        * bucket pushed to the far pile since it last moved, and the pile is
@@ -1379,6 +1387,7 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
           st_rlx32(&G->lh_dense, 0u);
           st_rlx32(&G->lh_k, 0u);
           st_rlx32(&G->hs_block, 0u);
+          st_rlx32(&G->wide, 0u);
         }
       } else if (ma | mb) {
         /* the nearest non-empty slot; with adaptation on, while the entries
@@ -1429,7 +1438,10 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
           }
           hsb = hsb || full != 0u;
         }
-        if (lane == 0) st_rlx32(&G->hs_block, hsb ? 1u : 0u);
+        if (lane == 0) {
+          st_rlx32(&G->hs_block, hsb ? 1u : 0u);
+          st_rlx32(&G->wide, nx != 0u ? 1u : 0u);
+        }
       } else {
         next_query = true;
       }
@@ -1471,7 +1483,6 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
       mode = PH_M_EXIT;
     }
   }
-  if (lane == 0 && pcs != pc_next) st_rlx32(&G->pc_state, pc_next);
   const unsigned long long wb = ld_rlx64(&G->work);
   unsigned epoch = prev_epoch; /* a records-only phase keeps its producer's */
   if (lane == 0 && !hub_only) {

@@ -144,15 +144,7 @@ struct __align__(128) PhGroup {
    * scan: it was already, or a light phase relaxed whole rows, or the
    * bucket was widened over several slots */
   unsigned hs_block;
-  /* pull or push for a settled bucket's heavy edges: a sampling heavy scan
-   * sums the heavy out-edges of the bucket (pc_push) and the in-edges of
-   * every vertex a heavy edge could still improve (pc_pull) over the same
-   * sample; pc_state is 1 while those sums belong to the decision about to
-   * be made, 2 right after it chose push (no second sample) */
-  unsigned pc_state;
-  unsigned pad5[12];
-  unsigned long long pc_push, pc_pull;
-  unsigned long long pad5b[14];
+  unsigned pad5[13];
   /* dense bucket slots (bit per slot): a slot whose pushes passed the dense
    * threshold stops storing entries; its bucket is collected by a scan of
    * the distances when it opens (PH_M_SCAN) */
@@ -164,6 +156,19 @@ struct __align__(128) PhGroup {
   unsigned long long pad6[14];
   unsigned long long head[PH_NLIST];
   PhTail tails[PH_NLIST];
+  /* pull or push for a settled bucket's heavy edges (kept after the other
+   * fields, which keep their offsets): a sampling heavy scan sums the heavy
+   * out-edges of the bucket (pc_push) and the in-edges of every vertex a
+   * heavy edge could still improve (pc_pull) over the same sample; pc_state
+   * is 1 while those sums belong to the decision about to be made, 2 right
+   * after it chose push (no second sample).  wide: the current bucket was
+   * widened over several slots, so its settled list holds vertices of lower
+   * buckets too (no pull). */
+  unsigned pc_state;
+  unsigned wide;
+  unsigned pad7[30];
+  unsigned long long pc_push, pc_pull;
+  unsigned long long pad8[14];
 };
 
 /* Engine-wide control and statistics. */
