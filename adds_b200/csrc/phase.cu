@@ -1033,8 +1033,9 @@ __device__ void pull_tile_warp(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S,
 
 
 /* ------------------------------------------------------------------------ */
-/* One phase (or, solo, the whole of it on this CTA).                         */
-template <bool FLT, int BLOCK, int UU>
+/* One phase (or, solo, the whole of it on this CTA).  PK: the kernel may
+ * pick pull phases (sampling scans compiled in). */
+template <bool FLT, int BLOCK, int UU, bool PK>
 __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool solo) {
   constexpr unsigned FLUSH_AT = PSmem<BLOCK, UU>::FLUSH_AT;
   const unsigned tid = threadIdx.x;
@@ -1073,7 +1074,7 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
      * the in-edges of the vertices above pull_floor. */
     constexpr unsigned SCANG = 4;
     const bool heavy = S.D.list == PH_LSETTLED;
-    const bool sample = heavy && S.D.sample != 0u;
+    const bool sample = PK && heavy && S.D.sample != 0u;
     const bool count = sample && Q.trow != nullptr;
     const unsigned tstep = sample ? PH_SAMPLE_STRIDE : 1u;
     const unsigned pfl = count ? pull_floor<FLT>(Q, S.D.base) : 0xFFFFFFFFu;
@@ -1185,8 +1186,9 @@ __device__ void run_phase(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, bool s
 /* ------------------------------------------------------------------------ */
 /* The leader's decision (warp 0 of the last CTA to reach the barrier): what
  * the group runs next.  Replaces the assign manager's bucket advance and
- * termination logic (wl.h:851-1527) with a read of the list tails. */
-template <bool FLT, int BLOCK, int UU>
+ * termination logic (wl.h:851-1527) with a read of the list tails.  PK: pull
+ * phases may be picked. */
+template <bool FLT, int BLOCK, int UU, bool PK>
 __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
   const unsigned lane = threadIdx.x & 31u;
   PhGroup *G = grp_of(P, c);
@@ -1277,7 +1279,8 @@ __device__ void leader_step(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S) {
        * taken as a pull when that reads fewer edges than the push */
       const PhQuery &Qh = P.qs[q];
       const unsigned long long thr = max(4096u, Qh.n >> (P.dense_shift ? P.dense_shift : 31u));
-      const bool pull_ok = P.pull_ok && Qh.trow != nullptr && Qh.split != nullptr && !P.near_far;
+      const bool pull_ok =
+          PK && P.pull_ok && Qh.trow != nullptr && Qh.split != nullptr && !P.near_far;
       const unsigned long long pull_thr = max(4096ull, (unsigned long long)(Qh.n >> 6));
       /* 1: the sampling scan just counted for this list; 2: it chose push
        * (no second sample).  Read only where a pull is possible. */
@@ -1607,7 +1610,11 @@ __device__ __forceinline__ bool solo_ok(const PhParams &P, const PSmem<BLOCK, UU
 /* edges in flight per thread: 8 where a thread may hold 128 registers, 4 at 64 */
 #define PH_U(BLOCK, MINB) ((BLOCK) * (MINB) >= 1024 ? 4 : 8)
 
-template <bool FLT, int BLOCK, int MINB>
+/* PK: an instantiation that may pick pull phases (P.pull_ok); the one
+ * without them is the same code with the sampling scans and the pull choice
+ * compiled out -- the extra code alone made the push loop about 7 % slower
+ * (R-MAT 24, batches), so launches that cannot pull do not carry it. */
+template <bool FLT, int BLOCK, int MINB, bool PK>
 __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constant__ PhParams P) {
   constexpr int UU = PH_U(BLOCK, MINB);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1642,7 +1649,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
   __syncthreads();
   while (S.D.mode != PH_M_EXIT) { /* left at the end of the body */
     if (tid == 0) S.tk = clock64();
-    run_phase<FLT, BLOCK, UU>(P, c, S, false);
+    run_phase<FLT, BLOCK, UU, PK>(P, c, S, false);
     if (tid == 0) { /* run_phase as a whole, grid phases */
       const long long t1 = clock64();
       S.cy[6] += (unsigned long long)(t1 - S.tk);
@@ -1665,7 +1672,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
     __syncthreads();
     if (S.leader) {
       for (;;) {
-        if (tid < 32) leader_step<FLT, BLOCK, UU>(P, c, S);
+        if (tid < 32) leader_step<FLT, BLOCK, UU, PK>(P, c, S);
         __syncthreads();
         if (tid == 0) ++S.nphase;
         if (!solo_ok<BLOCK, UU>(P, S)) break;
@@ -1680,7 +1687,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) phase_kernel(const __grid_constan
             if (i < P.trace_cap) P.trace[i].mode |= 0x100;
           }
         }
-        run_phase<FLT, BLOCK, UU>(P, c, S, true);
+        run_phase<FLT, BLOCK, UU, PK>(P, c, S, true);
         if (tracing) trace_account<BLOCK, UU>(P, c, S);
         __syncthreads();
       }
@@ -1793,14 +1800,27 @@ __global__ void __launch_bounds__(BLOCK, MINB) pull_kernel(const __grid_constant
 template <bool FLT, int BLOCK, int MINB>
 static cudaError_t prep_one(int *max_blocks_per_sm) {
   const size_t smem = sizeof(PSmem<BLOCK, PH_U(BLOCK, MINB)>);
-  cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB>,
+  cudaError_t e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB, false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(phase_kernel<FLT, BLOCK, MINB, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(pull_kernel<FLT, BLOCK, MINB>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks_per_sm,
-                                                       phase_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
+  /* the grid must be resident for every kernel of a launch chain */
+  int a = 0, b = 0, p = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, phase_kernel<FLT, BLOCK, MINB, false>,
+                                                    BLOCK, smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, phase_kernel<FLT, BLOCK, MINB, true>,
+                                                      BLOCK, smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, pull_kernel<FLT, BLOCK, MINB>, BLOCK, smem);
+  const int ab = a < b ? a : b;
+  *max_blocks_per_sm = ab < p ? ab : p;
+  return e;
 }
 
 template <bool FLT, int BLOCK, int MINB>
@@ -1818,8 +1838,9 @@ static cudaError_t launch_one(const PhParams &P, cudaStream_t st, bool pull) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return pull ? cudaLaunchKernelEx(&cfg, pull_kernel<FLT, BLOCK, MINB>, P)
-              : cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB>, P);
+  if (pull) return cudaLaunchKernelEx(&cfg, pull_kernel<FLT, BLOCK, MINB>, P);
+  return P.pull_ok ? cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB, true>, P)
+                   : cudaLaunchKernelEx(&cfg, phase_kernel<FLT, BLOCK, MINB, false>, P);
 }
 
 /* Failure-detection check: thread 0 waits, through the same bounded Waiter
