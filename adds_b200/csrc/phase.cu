@@ -835,8 +835,9 @@ __device__ void expand(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQ
  *
  * CTAs claim runs of tiles of PH_PULL_SUB x PH_PULL_V x BLOCK vertices (guided
  * self-scheduling, the next run claimed one run ahead; thread 0 keeps the
- * runs in shared memory) and run each through pull_tile.  Claims the next
- * tile into S.pl_cur; false when none is left.  Every thread calls it. */
+ * runs in shared memory) and run each sub-tile through pull_tile_warp.
+ * Claims the next tile into S.pl_cur; false when none is left.  Every
+ * thread calls it. */
 template <bool FLT, int BLOCK, int UU>
 __device__ bool prepare_pull(const PhParams &P, Ctx &c, PSmem<BLOCK, UU> &S, const PhQuery &Q) {
   const unsigned tid = threadIdx.x;
