@@ -67,6 +67,9 @@ def test_strerror_and_defaults():
     assert lib.adds_strerror(0) == b"ok"
     o = A.default_opts()
     assert o.delta_shift == -1 and o.window == 0 and o.light_heavy == -1 and o.local_max == -1
+    # pull phases: 0 = automatic (a field that was reserved, so callers that
+    # zero the struct get the automatic choice)
+    assert o.pull == 0 and list(o.reserved) == [0, 0]
 
 
 def test_invalid_arguments_return_codes():
